@@ -1,0 +1,450 @@
+"""Host-side Python mirror of the reference driver's interface to the hot path.
+
+The reference (AMR-LBM-OpenMP-2D, Fortran 90 + OpenMP) drives its solver
+from ``Main_Loop`` (AMR_Rising_2D_OMP.f90:267-377) by calling, in order,
+``Determine_Min_Max_Levels``, ``Fill_Ghost_Cells_C2``,
+``Phase_Field_LBM_h_g_AMR``, ``Macroscopic_Values_h_AMR``,
+``Fill_Ghost_Cells_C``, ``Macroscopic_Values_g_AMR`` and
+``Refine_Derefine_Mesh``. :class:`AmrLbm` exposes exactly those call sites
+(same names in snake case, same meaning) over the C ABI of ``libamrlbm.so``
+(``include/amrlbm.h``), whose kernels run on the B200. Every method raises
+:class:`AmrLbmError` with the library's message when the status is not 0;
+there is no CPU fallback: a missing library or device is an error.
+
+Field arrays use the reference's layouts (Parameters.f90:36-37) as numpy
+arrays in Fortran order: ``h, g`` (9, nx+2, ny+2), ``C`` (nx+4, ny+4),
+``P, Ux, Uy`` (nx, ny).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libamrlbm.so")
+
+# status codes (include/amrlbm.h)
+OK = 0
+ERR_ARG = 1
+ERR_CUDA = 2
+ERR_POOL_FULL = 3
+ERR_LEVEL_JUMP = 4
+ERR_NAN = 5
+ERR_DANGLING = 6
+ERR_STATE = 7
+ERR_TIMEOUT = 8
+
+F_LEAF, F_HASLEAF, F_REFIN, F_DEREF, F_ALLOC = 1, 2, 4, 8, 16
+
+
+class Params(ct.Structure):
+    """``amrlbm_params`` (include/amrlbm.h)."""
+
+    _fields_ = [
+        ("nx", ct.c_int32), ("ny", ct.c_int32),
+        ("nbx", ct.c_int32), ("nby", ct.c_int32),
+        ("dx0", ct.c_int32),
+        ("min_levels", ct.c_int32), ("max_levels", ct.c_int32),
+        ("max_blks", ct.c_int32),
+        ("regrid_every", ct.c_int32), ("reserved0", ct.c_int32),
+        ("rho_l", ct.c_double), ("rho_h", ct.c_double),
+        ("visc_ratio", ct.c_double),
+        ("bo", ct.c_double), ("ar", ct.c_double),
+        ("gy", ct.c_double),
+        ("w", ct.c_double), ("m0", ct.c_double),
+        ("radius", ct.c_double), ("xc", ct.c_double), ("yc", ct.c_double),
+        ("refin_tol", ct.c_double), ("deref_tol", ct.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved0"}
+
+
+class Physics(ct.Structure):
+    """``amrlbm_physics`` (include/amrlbm.h), D2Q9_Mod.f90:13-16."""
+
+    _fields_ = [(k, ct.c_double) for k in
+                ("w", "sigma", "beta", "kappa", "tau_l", "tau_h", "rho_l", "rho_h", "gy", "m0")]
+
+
+def reference_params() -> Params:
+    """The reference's compile-time configuration: nx=ny=8, L0=256, three base
+    blocks stacked in y, minLevels=1, maxLevels=log2(L0/nx)=5,
+    MaxBlks=6*(L0/nx)**2 (Parameters.f90:12-19); rho 0.001/1, Bo=Ar=40,
+    Gy=5e-6, W=5, M0=0.03, R=L0/10 at (L0/2, L0/2), tolerances 0.002/0.001
+    (AMR_Rising_2D_OMP.f90:154-158,241-259,276-277, D2Q9_Mod.f90:10)."""
+    L0, nx = 256, 8
+    return Params(nx=nx, ny=nx, nbx=1, nby=3, dx0=L0 // nx, min_levels=1,
+                  max_levels=int(round(math.log(L0 // nx) / math.log(2.0))),
+                  max_blks=6 * (L0 // nx) ** 2, regrid_every=1,
+                  rho_l=0.001, rho_h=1.0, visc_ratio=100.0, bo=40.0, ar=40.0,
+                  gy=0.000005, w=5.0, m0=0.03, radius=L0 / 10.0, xc=float(L0 // 2),
+                  yc=float(L0 // 2), refin_tol=0.002, deref_tol=0.001)
+
+
+def archimedes(eo: float, mo: float) -> float:
+    """Ar = (Eo^3/Mo)^(1/4): the reference parameterises buoyancy by Bo (=Eo)
+    and Ar (AMR_Rising_2D_OMP.f90:244-250)."""
+    return (eo ** 3 / mo) ** 0.25
+
+
+def tree_blocks(nbx: int, nby: int, levels: int) -> int:
+    """Blocks of a fully refined quadtree over nbx x nby base blocks: an upper
+    bound of the pool size the regrid can ever need."""
+    return sum(nbx * nby * 4 ** l for l in range(levels + 1))
+
+
+def bubble_params(base_x: int, base_y: int, levels: int, radius: float, xc: float,
+                  yc: float, rho_ratio: float, visc_ratio: float, eo: float, mo: float,
+                  w: float = 4.0, m0: float = 0.02, refin_tol: float = 1e-3,
+                  deref_tol: float = 5e-4, regrid_every: int = 1, n: int = 16,
+                  max_blks: int | None = None) -> Params:
+    """A rising-bubble workload on a base grid of base_x x base_y cells in
+    n x n blocks with `levels` refinement levels above the base (finest cell =
+    1 length unit, so the base cell size is 2**levels). minLevels = 0: base
+    blocks may stay leaves."""
+    assert base_x % n == 0 and base_y % n == 0
+    nbx, nby = base_x // n, base_y // n
+    if max_blks is None:
+        max_blks = tree_blocks(nbx, nby, levels)
+    return Params(nx=n, ny=n, nbx=nbx, nby=nby, dx0=2 ** levels, min_levels=0,
+                  max_levels=levels, max_blks=max_blks, regrid_every=regrid_every,
+                  rho_l=1.0 / rho_ratio, rho_h=1.0, visc_ratio=visc_ratio, bo=eo,
+                  ar=archimedes(eo, mo), gy=0.000005, w=w, m0=m0, radius=radius,
+                  xc=xc, yc=yc, refin_tol=refin_tol, deref_tol=deref_tol)
+
+
+def workload_small() -> Params:
+    """Plain FP64 rising bubble: base grid 64x128 cells in 16x16 blocks, 2
+    refinement levels (finest-equivalent 256x512), R=32 at (128,128),
+    density ratio 10, viscosity ratio 10, Eo=10, Mo=1e-3, W=4, M=0.02,
+    refine where |grad C| > 1e-3 (derefine tolerance 5e-4, half the refine
+    tolerance as in the reference's 0.002/0.001)."""
+    return bubble_params(64, 128, 2, 32.0, 128.0, 128.0, 10.0, 10.0, 10.0, 1e-3,
+                         w=4.0, m0=0.02, refin_tol=1e-3, deref_tol=5e-4, regrid_every=1)
+
+
+def workload_large() -> Params:
+    """Plain FP64 rising bubble at scale: base grid 256x512 cells in 16x16
+    blocks, 3 refinement levels (finest-equivalent 2048x4096), R=128 at
+    (1024,512), density ratio 1000, viscosity ratio 100, Eo=10, Mo=1e-5, W=4,
+    regrid every 10 steps (mobility and tolerances as the small workload)."""
+    return bubble_params(256, 512, 3, 128.0, 1024.0, 512.0, 1000.0, 100.0, 10.0, 1e-5,
+                         w=4.0, m0=0.02, refin_tol=1e-3, deref_tol=5e-4, regrid_every=10)
+
+
+class AmrLbmError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"amrlbm status {status}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Loads libamrlbm.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise AmrLbmError(ERR_STATE, f"{p} not built (run make in {_HERE})")
+    lib = ct.CDLL(p)
+    i32p = ct.POINTER(ct.c_int32)
+    dp = ct.POINTER(ct.c_double)
+    u8p = ct.POINTER(ct.c_uint8)
+    vp = ct.c_void_p
+    sig = {
+        "amrlbm_default_params": (None, [ct.POINTER(Params)]),
+        "amrlbm_derive_physics": (ct.c_int, [ct.POINTER(Params), ct.POINTER(Physics)]),
+        "amrlbm_create": (ct.c_int, [ct.POINTER(Params), ct.POINTER(vp)]),
+        "amrlbm_destroy": (ct.c_int, [vp]),
+        "amrlbm_set_physics": (ct.c_int, [vp, ct.POINTER(Physics)]),
+        "amrlbm_last_error": (ct.c_char_p, [vp]),
+        "amrlbm_device_bytes": (ct.c_int64, [vp]),
+        "amrlbm_get_counts": (ct.c_int, [vp, i32p]),
+        "amrlbm_set_level_range": (ct.c_int, [vp, ct.c_int32, ct.c_int32]),
+        "amrlbm_set_topology": (ct.c_int, [vp, ct.c_int32, i32p, i32p, i32p, i32p, i32p,
+                                           i32p, i32p, i32p, u8p, ct.c_int32, i32p,
+                                           ct.c_int32]),
+        "amrlbm_get_topology": (ct.c_int, [vp, i32p, i32p, i32p, i32p, i32p, i32p, i32p,
+                                           i32p, u8p, i32p, i32p]),
+        "amrlbm_get_neighbours": (ct.c_int, [vp, i32p]),
+        "amrlbm_get_leaves": (ct.c_int, [vp, i32p]),
+        "amrlbm_upload_block": (ct.c_int, [vp, ct.c_int32, dp, dp, dp, dp, dp, dp]),
+        "amrlbm_download_block": (ct.c_int, [vp, ct.c_int32, dp, dp, dp, dp, dp, dp]),
+        "amrlbm_upload_fields": (ct.c_int, [vp, ct.c_int32, i32p, dp, dp, dp, dp, dp, dp]),
+        "amrlbm_download_fields": (ct.c_int, [vp, ct.c_int32, i32p, dp, dp, dp, dp, dp, dp]),
+        "amrlbm_get_block_error": (ct.c_int, [vp, dp]),
+        "amrlbm_init_rising_bubble": (ct.c_int, [vp]),
+        "amrlbm_init_fields": (ct.c_int, [vp]),
+        "amrlbm_min_max_levels": (ct.c_int, [vp, i32p, i32p]),
+        "amrlbm_fill_ghost_c2": (ct.c_int, [vp]),
+        "amrlbm_phase_field_step": (ct.c_int, [vp]),
+        "amrlbm_macro_h": (ct.c_int, [vp]),
+        "amrlbm_fill_ghost_c": (ct.c_int, [vp]),
+        "amrlbm_macro_g": (ct.c_int, [vp]),
+        "amrlbm_regrid": (ct.c_int, [vp, ct.c_double, ct.c_double]),
+        "amrlbm_step": (ct.c_int, [vp, ct.c_int32]),
+        "amrlbm_sync": (ct.c_int, [vp]),
+        "amrlbm_diag": (ct.c_int, [vp, dp]),
+        "amrlbm_timer_start": (ct.c_int, [vp]),
+        "amrlbm_timer_stop": (ct.c_int, [vp, ct.POINTER(ct.c_float)]),
+        "amrlbm_profile_enable": (ct.c_int, [vp, ct.c_int32]),
+        "amrlbm_profile_read": (ct.c_int, [vp, ct.c_int32, dp, ct.POINTER(ct.c_int64),
+                                           ct.POINTER(ct.c_int64)]),
+        "amrlbm_launch_count": (ct.c_int64, [vp]),
+        "amrlbm_flush_l2": (ct.c_int, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    """Names of every entry point declared in include/amrlbm.h."""
+    hdr = os.path.join(_HERE, "..", "include", "amrlbm.h")
+    import re
+    names = []
+    with open(hdr) as f:
+        for line in f:
+            m = re.match(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(amrlbm_\w+)\s*\(", line)
+            if m:
+                names.append(m.group(1))
+    return names
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ct.POINTER(ctype))
+
+
+class AmrLbm:
+    """One device-resident block pool, driven like the reference's Main_Loop."""
+
+    def __init__(self, params: Params, lib=None):
+        self.lib = lib or load_library()
+        self.params = params
+        self.nx, self.ny = params.nx, params.ny
+        ctx = ct.c_void_p()
+        st = self.lib.amrlbm_create(ct.byref(params), ct.byref(ctx))
+        if st != 0:
+            raise AmrLbmError(st, "amrlbm_create failed (is a B200 visible?)")
+        self.ctx = ctx
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, st):
+        if st != 0:
+            msg = self.lib.amrlbm_last_error(self.ctx)
+            raise AmrLbmError(st, msg.decode() if msg else "")
+        return st
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.amrlbm_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def hshape(self):
+        return (9, self.nx + 2, self.ny + 2)
+
+    @property
+    def cshape(self):
+        return (self.nx + 4, self.ny + 4)
+
+    @property
+    def pshape(self):
+        return (self.nx, self.ny)
+
+    # -- driver ------------------------------------------------------------
+    def initialize_rising_bubble(self):
+        """AMR_LBM_Rising_Bubble start-up (AMR_Rising_2D_OMP.f90:49-67)."""
+        self._check(self.lib.amrlbm_init_rising_bubble(self.ctx))
+
+    def initialize_fields(self):
+        """Initialize_AMR_Rising_Bubble (AMR_Rising_2D_OMP.f90:142-231)."""
+        self._check(self.lib.amrlbm_init_fields(self.ctx))
+
+    def set_physics(self, phys: Physics):
+        self._check(self.lib.amrlbm_set_physics(self.ctx, ct.byref(phys)))
+
+    # -- Main_Loop call sites ---------------------------------------------
+    def determine_min_max_levels(self):
+        lo, hi = ct.c_int32(), ct.c_int32()
+        self._check(self.lib.amrlbm_min_max_levels(self.ctx, ct.byref(lo), ct.byref(hi)))
+        return lo.value, hi.value
+
+    def set_level_range(self, lmin, lmax):
+        self._check(self.lib.amrlbm_set_level_range(self.ctx, lmin, lmax))
+
+    def fill_ghost_cells_c2(self):
+        self._check(self.lib.amrlbm_fill_ghost_c2(self.ctx))
+
+    def phase_field_lbm_h_g(self):
+        self._check(self.lib.amrlbm_phase_field_step(self.ctx))
+
+    def macroscopic_values_h(self):
+        self._check(self.lib.amrlbm_macro_h(self.ctx))
+
+    def fill_ghost_cells_c(self):
+        self._check(self.lib.amrlbm_fill_ghost_c(self.ctx))
+
+    def macroscopic_values_g(self):
+        self._check(self.lib.amrlbm_macro_g(self.ctx))
+
+    def refine_derefine_mesh(self, refin_tol=None, deref_tol=None):
+        rt = self.params.refin_tol if refin_tol is None else refin_tol
+        dt = self.params.deref_tol if deref_tol is None else deref_tol
+        self._check(self.lib.amrlbm_regrid(self.ctx, rt, dt))
+
+    def main_loop(self, nsteps: int):
+        """nsteps iterations of the Main_Loop body (fused, graph-captured)."""
+        self._check(self.lib.amrlbm_step(self.ctx, nsteps))
+
+    def sync(self):
+        self._check(self.lib.amrlbm_sync(self.ctx))
+
+    def output(self):
+        """Output (AMR_Rising_2D_OMP.f90:456-489) + bubble centroid/rise velocity."""
+        out = np.zeros(8)
+        self._check(self.lib.amrlbm_diag(self.ctx, _ptr(out, ct.c_double)))
+        return dict(zip(("mass", "rho_min", "rho_max", "u_max", "bubble_volume",
+                         "y_centroid", "rise_velocity", "phase_volume"), out.tolist()))
+
+    # -- state -------------------------------------------------------------
+    def counts(self):
+        c = np.zeros(5, dtype=np.int32)
+        self._check(self.lib.amrlbm_get_counts(self.ctx, _ptr(c, ct.c_int32)))
+        return dict(zip(("nblks", "nleaf", "kk", "level_min", "level_max"), c.tolist()))
+
+    def topology(self):
+        n = self.counts()["nblks"]
+        i32 = lambda k=1: np.zeros(n * k, dtype=np.int32)
+        t = dict(level=i32(), dx=i32(), bi=i32(), bj=i32(), parent=i32(), child=i32(4),
+                 nbr_owner=i32(8), nbr_slot=i32(8), flags=np.zeros(n, dtype=np.uint8))
+        nfree = ct.c_int32()
+        fl = np.zeros(self.params.max_blks // 4 + 1, dtype=np.int32)
+        self._check(self.lib.amrlbm_get_topology(
+            self.ctx, *[_ptr(t[k], ct.c_int32) for k in
+                        ("level", "dx", "bi", "bj", "parent", "child", "nbr_owner",
+                         "nbr_slot")],
+            _ptr(t["flags"], ct.c_uint8), ct.byref(nfree), _ptr(fl, ct.c_int32)))
+        t["free_list"] = fl[: nfree.value].copy()
+        t["child"] = t["child"].reshape(n, 4)
+        t["nbr_owner"] = t["nbr_owner"].reshape(n, 8)
+        t["nbr_slot"] = t["nbr_slot"].reshape(n, 8)
+        return t
+
+    def set_topology(self, t, kk):
+        n = len(t["level"])
+        c = lambda a: np.ascontiguousarray(a, dtype=np.int32).ravel()
+        arrs = [c(t[k]) for k in ("level", "dx", "bi", "bj", "parent", "child",
+                                  "nbr_owner", "nbr_slot")]
+        flags = np.ascontiguousarray(t["flags"], dtype=np.uint8)
+        fl = c(t["free_list"]) if len(t["free_list"]) else np.zeros(1, np.int32)
+        self._check(self.lib.amrlbm_set_topology(
+            self.ctx, n, *[_ptr(a, ct.c_int32) for a in arrs], _ptr(flags, ct.c_uint8),
+            len(t["free_list"]), _ptr(fl, ct.c_int32), kk))
+
+    def neighbours(self):
+        n = self.counts()["nblks"]
+        a = np.zeros(8 * n, dtype=np.int32)
+        self._check(self.lib.amrlbm_get_neighbours(self.ctx, _ptr(a, ct.c_int32)))
+        return a.reshape(n, 8)
+
+    def leaves(self):
+        n = self.counts()["nleaf"]
+        a = np.zeros(max(n, 1), dtype=np.int32)
+        self._check(self.lib.amrlbm_get_leaves(self.ctx, _ptr(a, ct.c_int32)))
+        return a[:n]
+
+    def block_errors(self):
+        n = self.counts()["nblks"]
+        a = np.zeros(n)
+        self._check(self.lib.amrlbm_get_block_error(self.ctx, _ptr(a, ct.c_double)))
+        return a
+
+    def download_block(self, bid):
+        h = np.zeros(self.hshape, order="F")
+        g = np.zeros(self.hshape, order="F")
+        C = np.zeros(self.cshape, order="F")
+        P = np.zeros(self.pshape, order="F")
+        Ux = np.zeros(self.pshape, order="F")
+        Uy = np.zeros(self.pshape, order="F")
+        self._check(self.lib.amrlbm_download_block(
+            self.ctx, bid, *[_ptr(a, ct.c_double) for a in (h, g, C, P, Ux, Uy)]))
+        return dict(h=h, g=g, C=C, P=P, Ux=Ux, Uy=Uy)
+
+    def upload_block(self, bid, h=None, g=None, C=None, P=None, Ux=None, Uy=None):
+        f = lambda a: None if a is None else np.asfortranarray(a, dtype=np.float64)
+        arrs = [f(a) for a in (h, g, C, P, Ux, Uy)]
+        self._check(self.lib.amrlbm_upload_block(
+            self.ctx, bid, *[_ptr(a, ct.c_double) for a in arrs]))
+
+    def download_fields(self, ids):
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        n = len(ids)
+        out = dict(h=np.zeros((n,) + self.hshape[::-1]), g=np.zeros((n,) + self.hshape[::-1]),
+                   C=np.zeros((n,) + self.cshape[::-1]), P=np.zeros((n,) + self.pshape[::-1]),
+                   Ux=np.zeros((n,) + self.pshape[::-1]), Uy=np.zeros((n,) + self.pshape[::-1]))
+        self._check(self.lib.amrlbm_download_fields(
+            self.ctx, n, _ptr(ids, ct.c_int32),
+            *[_ptr(out[k], ct.c_double) for k in ("h", "g", "C", "P", "Ux", "Uy")]))
+        return out
+
+    def upload_fields(self, ids, fields):
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        arrs = [None if fields.get(k) is None else np.ascontiguousarray(fields[k], np.float64)
+                for k in ("h", "g", "C", "P", "Ux", "Uy")]
+        self._check(self.lib.amrlbm_upload_fields(
+            self.ctx, len(ids), _ptr(ids, ct.c_int32), *[_ptr(a, ct.c_double) for a in arrs]))
+
+    # -- timing ------------------------------------------------------------
+    def timer_start(self):
+        self._check(self.lib.amrlbm_timer_start(self.ctx))
+
+    def timer_stop(self) -> float:
+        ms = ct.c_float()
+        self._check(self.lib.amrlbm_timer_stop(self.ctx, ct.byref(ms)))
+        return ms.value
+
+    def profile(self, enable: bool):
+        self._check(self.lib.amrlbm_profile_enable(self.ctx, 1 if enable else 0))
+
+    def profile_read(self, kernel: int = 0):
+        t = ct.c_double()
+        n = ct.c_int64()
+        cells = ct.c_int64()
+        self._check(self.lib.amrlbm_profile_read(self.ctx, kernel, ct.byref(t), ct.byref(n),
+                                                 ct.byref(cells)))
+        return t.value, n.value, cells.value
+
+    def launch_count(self) -> int:
+        return int(self.lib.amrlbm_launch_count(self.ctx))
+
+    def flush_l2(self):
+        self._check(self.lib.amrlbm_flush_l2(self.ctx))
+
+    def device_bytes(self) -> int:
+        return int(self.lib.amrlbm_device_bytes(self.ctx))

@@ -1,0 +1,1014 @@
+// amrlbm_api.cu - the extern "C" boundary (include/amrlbm.h): context and
+// device block pool, host<->device transfers in the reference's layouts, the
+// driver's start-up, CUDA-graph stepping, diagnostics and timing.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "amrlbm.h"
+#include "amrlbm_launch.h"
+
+namespace {
+
+size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof;  // (kernel, events)
+};
+
+}  // namespace
+
+struct amrlbm_ctx {
+    amrlbm_params prm{};
+    DevState s{};
+    LaunchCfg lc{};
+    cudaStream_t st = nullptr;
+    std::string err;
+    int64_t bytes = 0;
+    long long stepcount = 0;
+    bool tail_done = true;  // P,U and C ring 1 of the current state are materialised
+    std::vector<void*> allocs;
+    double* d_diag = nullptr;
+    double* d_stage = nullptr;
+    size_t stage_doubles = 0;
+    int* d_ids = nullptr;
+    size_t ids_cap = 0;
+    void* d_flush = nullptr;
+    size_t flush_bytes = 0;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    bool prof = false;
+    double prof_ms[4] = {0, 0, 0, 0};
+    long long prof_n[4] = {0, 0, 0, 0};
+    long long prof_cells[4] = {0, 0, 0, 0};
+    std::map<std::tuple<int, int, int, int, int>, GraphEntry> graphs;
+    long long launches0 = 0;
+};
+
+namespace {
+
+int fail(amrlbm_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(amrlbm_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, AMRLBM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+template <class T>
+T* dalloc(amrlbm_ctx* ctx, size_t n, cudaError_t* e) {
+    void* p = nullptr;
+    *e = cudaMalloc(&p, n * sizeof(T));
+    if (*e == cudaSuccess) {
+        cudaMemset(p, 0, n * sizeof(T));
+        ctx->allocs.push_back(p);
+        ctx->bytes += (int64_t)(n * sizeof(T));
+    }
+    return (T*)p;
+}
+
+PhysD to_physd(const amrlbm_physics& p) {
+    PhysD d;
+    d.W = p.w;
+    d.Sigma = p.sigma;
+    d.Beta = p.beta;
+    d.kappa = p.kappa;
+    d.taul = p.tau_l;
+    d.tauh = p.tau_h;
+    d.Rhol = p.rho_l;
+    d.Rhoh = p.rho_h;
+    d.Gy = p.gy;
+    d.M0 = p.m0;
+    d.wc = 1.0 / (0.5 + d.M0 * 3.0);  // D2Q9_Mod.f90:11
+    return d;
+}
+
+// ---- field transfer kernels (reference layouts <-> pool layouts) ----------
+// per block record offsets in the staging buffer
+struct StageLayout {
+    size_t h, g, C, P, Ux, Uy, per;
+};
+StageLayout stage_layout(int nx, int ny) {
+    StageLayout L;
+    const size_t hs = (size_t)9 * (nx + 2) * (ny + 2), cs = (size_t)(nx + 4) * (ny + 4),
+                 ps = (size_t)nx * ny;
+    L.h = 0;
+    L.g = hs;
+    L.C = 2 * hs;
+    L.P = 2 * hs + cs;
+    L.Ux = L.P + ps;
+    L.Uy = L.Ux + ps;
+    L.per = L.Uy + ps;
+    return L;
+}
+
+// dir 0: staging (reference layout) -> pool; 1: pool -> staging. mask bits: h g C P Ux Uy
+__global__ void k_transfer(DevState s, const int* ids, int n, double* stage, int dir, int mask,
+                           StageLayout L) {
+    const int nx = s.nx, ny = s.ny;
+    const int hs = 9 * (nx + 2) * (ny + 2), cs = (nx + 4) * (ny + 4), ps = nx * ny;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int b = ids[i];
+        double* rec = stage + (size_t)i * L.per;
+        for (int f = 0; f < 2; ++f) {
+            if (!(mask & (1 << f))) continue;
+            double* A = f ? s.Ag : s.Ah;
+            double* B = f ? s.Bg : s.Bh;
+            double* r = rec + (f ? L.g : L.h);
+            for (int e = threadIdx.x; e < hs; e += blockDim.x) {
+                const int q = e % 9 + 1, xy = e / 9, x = xy % (nx + 2), y = xy / (nx + 2);
+                const bool in = x >= 1 && x <= nx && y >= 1 && y <= ny;
+                double* p = in ? &B[b_idx(s, b, q, x, y)] : &A[a_idx(s, b, q, x, y)];
+                if (dir == 0)
+                    *p = r[e];
+                else
+                    r[e] = *p;
+            }
+        }
+        if (mask & 4)
+            for (int e = threadIdx.x; e < cs; e += blockDim.x) {
+                const int x = e % (nx + 4) - 1, y = e / (nx + 4) - 1;
+                double* p = &s.C[c_idx(s, b, x, y)];
+                if (dir == 0)
+                    *p = rec[L.C + e];
+                else
+                    rec[L.C + e] = *p;
+            }
+        for (int f = 0; f < 3; ++f) {
+            if (!(mask & (8 << f))) continue;
+            double* A = f == 0 ? s.P : (f == 1 ? s.Ux : s.Uy);
+            const size_t off = f == 0 ? L.P : (f == 1 ? L.Ux : L.Uy);
+            for (int e = threadIdx.x; e < ps; e += blockDim.x) {
+                double* p = &A[(size_t)b * s.pplane + e];
+                if (dir == 0)
+                    *p = rec[off + e];
+                else
+                    rec[off + e] = *p;
+            }
+        }
+    }
+}
+
+int ensure_stage(amrlbm_ctx* ctx, size_t nblocks) {
+    const StageLayout L = stage_layout(ctx->prm.nx, ctx->prm.ny);
+    const size_t need = nblocks * L.per;
+    if (need > ctx->stage_doubles) {
+        if (ctx->d_stage) cudaFree(ctx->d_stage);
+        ctx->d_stage = nullptr;
+        CK(cudaMalloc(&ctx->d_stage, need * sizeof(double)));
+        ctx->stage_doubles = need;
+    }
+    if (nblocks > ctx->ids_cap) {
+        if (ctx->d_ids) cudaFree(ctx->d_ids);
+        ctx->d_ids = nullptr;
+        CK(cudaMalloc(&ctx->d_ids, nblocks * sizeof(int)));
+        ctx->ids_cap = nblocks;
+    }
+    return 0;
+}
+
+int device_error(amrlbm_ctx* ctx) {
+    int e[2] = {0, 0};
+    CK(cudaMemcpy(e, &ctx->s.cnt->error, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+    if (e[0] == 0) return 0;
+    const int zero[2] = {0, 0};
+    CK(cudaMemcpy(&ctx->s.cnt->error, zero, 2 * sizeof(int), cudaMemcpyHostToDevice));
+    static const char* names[] = {"ok", "argument", "cuda", "pool full (MaxBlks exceeded)",
+                                  "level jump > 1 between neighbours", "non-finite value",
+                                  "neighbour pointer into a freed block", "state",
+                                  "bounded device wait ran out"};
+    const char* nm = (e[0] >= 0 && e[0] <= 8) ? names[e[0]] : "unknown";
+    return fail(ctx, e[0], std::string("device: ") + nm + " (info " + std::to_string(e[1]) + ")");
+}
+
+int sync_check(amrlbm_ctx* ctx) {
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaGetLastError());
+    return device_error(ctx);
+}
+
+Counters read_counters(amrlbm_ctx* ctx) {
+    Counters c;
+    cudaMemcpy(&c, ctx->s.cnt, sizeof(Counters), cudaMemcpyDeviceToHost);
+    return c;
+}
+
+// Refine_Derefine_Mesh as a fixed launch sequence (graph-capturable).
+void enqueue_regrid(amrlbm_ctx* ctx, double rt, double dt, bool with_err, bool set_levels) {
+    const DevState& s = ctx->s;
+    if (with_err) launch_err(s, ctx->lc, ctx->st);
+    launch_regrid_flags(s, ctx->st, rt, dt);
+    launch_restrict(s, ctx->lc, ctx->st);
+    launch_regrid_topo(s, ctx->st, 0, -1, -1, set_levels ? 1 : 0);
+    launch_prolong(s, ctx->lc, ctx->st);
+}
+
+// one Main_Loop iteration. consumer of K1 depends on whether the previous
+// step materialised P,U; tail = Fill_Ghost_Cells_C + Macroscopic_Values_g_AMR.
+struct ProfMark {
+    amrlbm_ctx* ctx;
+    GraphEntry* ge;
+    int kernel;
+    cudaEvent_t a = nullptr;
+    ProfMark(amrlbm_ctx* c, GraphEntry* g, int k) : ctx(c), ge(g), kernel(k) {
+        if (ge && ctx->prof) {
+            cudaEvent_t b;
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecordWithFlags(a, ctx->st, cudaEventRecordExternal);
+            ge->prof.push_back({kernel, {a, b}});
+        }
+    }
+    ~ProfMark() {
+        if (ge && ctx->prof) cudaEventRecordWithFlags(ge->prof.back().second.second, ctx->st,
+                                                      cudaEventRecordExternal);
+    }
+};
+
+void enqueue_step(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail, bool regrid) {
+    const DevState& s = ctx->s;
+    {
+        ProfMark m(ctx, ge, 0);
+        launch_fill_c(s, ctx->lc, ctx->st, 2, prev_tail ? CONS_COLLIDE_READ : CONS_COLLIDE_FUSED);
+    }
+    {
+        ProfMark m(ctx, ge, 1);
+        launch_fill_hg_stream(s, ctx->lc, ctx->st);
+    }
+    if (tail) {
+        ProfMark m(ctx, ge, 2);
+        launch_fill_c(s, ctx->lc, ctx->st, 1, CONS_MACRO_G);
+    }
+    if (regrid) {
+        ProfMark m(ctx, ge, 3);
+        enqueue_regrid(ctx, ctx->prm.refin_tol, ctx->prm.deref_tol, false, true);
+    }
+}
+
+int set_level_counters(amrlbm_ctx* ctx, int lmin, int lmax) {
+    int v[2] = {lmin, lmax};
+    CK(cudaMemcpyAsync(&ctx->s.cnt->level_min, v, 2 * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return 0;
+}
+
+// host copy of the topology arrays for blocks 1..nb (index id)
+struct HostTopo {
+    std::vector<int> level, dx, bi, bj;
+};
+int get_leaves_host(amrlbm_ctx* ctx, std::vector<int>& leaves, HostTopo& t) {
+    Counters c = read_counters(ctx);
+    leaves.resize(c.nleaf);
+    if (c.nleaf)
+        CK(cudaMemcpy(leaves.data(), ctx->s.leaf, c.nleaf * sizeof(int), cudaMemcpyDeviceToHost));
+    const size_t nb = (size_t)c.nblks + 1;
+    t.level.resize(nb);
+    t.dx.resize(nb);
+    t.bi.resize(nb);
+    t.bj.resize(nb);
+    CK(cudaMemcpy(t.level.data(), ctx->s.level, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(t.dx.data(), ctx->s.dx, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(t.bi.data(), ctx->s.bi, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(t.bj.data(), ctx->s.bj, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int upload_blocks(amrlbm_ctx* ctx, int n, const int* ids, const double* h, const double* g,
+                  const double* C, const double* P, const double* Ux, const double* Uy);
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+void amrlbm_default_params(amrlbm_params* p) {
+    const int L0 = 256, nx = 8;
+    std::memset(p, 0, sizeof(*p));
+    p->nx = nx;
+    p->ny = nx;
+    p->nbx = 1;
+    p->nby = 3;
+    p->dx0 = L0 / nx;
+    p->min_levels = 1;
+    p->max_levels = (int)std::lround(std::log((double)(L0 / nx)) / std::log(2.0));
+    p->max_blks = 6 * (L0 / nx) * (L0 / nx);
+    p->regrid_every = 1;
+    p->rho_l = 0.001;
+    p->rho_h = 1.0;
+    p->visc_ratio = 100.0;
+    p->bo = 40.0;
+    p->ar = 40.0;
+    p->gy = 0.000005;
+    p->w = 5.0;
+    p->m0 = 0.03;
+    p->radius = L0 / 10.0;
+    p->xc = L0 / 2;
+    p->yc = L0 / 2;
+    p->refin_tol = 0.002;
+    p->deref_tol = 0.001;
+}
+
+// Set_Rising_Bubble_Parameters (AMR_Rising_2D_OMP.f90:235-263)
+int amrlbm_derive_physics(const amrlbm_params* p, amrlbm_physics* o) {
+    if (!p || !o) return AMRLBM_ERR_ARG;
+    const double R = p->radius;
+    const double D = 2.0 * R;
+    o->rho_l = p->rho_l;
+    o->rho_h = p->rho_h;
+    o->gy = p->gy;
+    o->sigma = o->gy * (o->rho_h - o->rho_l) * (D * D) / p->bo;
+    const double muh = std::sqrt(o->gy * o->rho_h * (o->rho_h - o->rho_l) * ((D * D) * D)) / p->ar;
+    const double mul = muh / p->visc_ratio;
+    o->tau_h = 3.0 * (muh / o->rho_h);
+    o->tau_l = 3.0 * (mul / o->rho_l);
+    o->w = p->w;
+    o->beta = 12.0 * o->sigma / o->w;
+    o->kappa = 1.5 * o->sigma * o->w;
+    o->m0 = p->m0;
+    return AMRLBM_OK;
+}
+
+int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
+    if (!p || !out) return AMRLBM_ERR_ARG;
+    *out = nullptr;
+    if (p->nx < 4 || p->ny < 4 || (p->nx % 2) || (p->ny % 2) || p->nx * p->ny > 1024 ||
+        p->nbx < 1 || p->nby < 1 || p->dx0 < 1 || p->min_levels < 0 ||
+        p->max_levels < p->min_levels || p->max_levels >= AMR_MAXLV - 1 || p->max_blks < 1 ||
+        p->max_blks < p->nbx * p->nby)
+        return AMRLBM_ERR_ARG;
+    if ((p->dx0 >> p->max_levels) < 1) return AMRLBM_ERR_ARG;  // dx stays an integer >= 1
+    int dev = 0, cc = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return AMRLBM_ERR_CUDA;
+    cudaDeviceGetAttribute(&cc, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cc != 10) return AMRLBM_ERR_CUDA;  // built for sm_100a only
+    amrlbm_ctx* ctx = new amrlbm_ctx();
+    ctx->prm = *p;
+    if (ctx->prm.regrid_every < 1) ctx->prm.regrid_every = 1;
+    DevState& s = ctx->s;
+    const int nx = p->nx, ny = p->ny;
+    s.nx = nx;
+    s.ny = ny;
+    s.max_blks = p->max_blks;
+    s.fl_cap = p->max_blks / 4 + 2;
+    s.ap = (int)round_up(nx + 5, 4);
+    s.aplane = (int)round_up((size_t)(ny + 2) * s.ap, 16);
+    s.bplane = nx * ny;
+    s.cp = (int)round_up(nx + 6, 4);
+    s.cplane = (int)round_up((size_t)(ny + 4) * s.cp, 16);
+    s.pplane = nx * ny;
+    s.min_levels = p->min_levels;
+    s.max_levels = p->max_levels;
+    amrlbm_physics ph;
+    amrlbm_derive_physics(p, &ph);
+    s.ph = to_physd(ph);
+    const size_t NB = (size_t)p->max_blks + 1;
+    cudaError_t e = cudaSuccess;
+#define AL(field, T, n)                                            \
+    s.field = dalloc<T>(ctx, (n), &e);                             \
+    if (e != cudaSuccess) {                                        \
+        int r = cuda_fail(ctx, e, "cudaMalloc " #field);           \
+        amrlbm_destroy(ctx);                                       \
+        return r;                                                  \
+    }
+    AL(Ah, double, NB * 9 * s.aplane);
+    AL(Ag, double, NB * 9 * s.aplane);
+    AL(Bh, double, NB * 9 * s.bplane);
+    AL(Bg, double, NB * 9 * s.bplane);
+    AL(C, double, NB * s.cplane);
+    AL(P, double, NB * s.pplane);
+    AL(Ux, double, NB * s.pplane);
+    AL(Uy, double, NB * s.pplane);
+    AL(err, double, NB);
+    AL(level, int, NB);
+    AL(dx, int, NB);
+    AL(bi, int, NB);
+    AL(bj, int, NB);
+    AL(parent, int, NB);
+    AL(child, int, 4 * NB);
+    AL(nb_owner, int, 8 * NB);
+    AL(nb_slot, int, 8 * NB);
+    AL(nb_gen, int, 8 * NB);
+    AL(gen, int, NB);
+    AL(nbr, int, 8 * NB);
+    AL(is_leaf, uint8_t, NB);
+    AL(has_leaf, uint8_t, NB);
+    AL(refin, uint8_t, NB);
+    AL(deref, uint8_t, NB);
+    AL(alloc, uint8_t, NB);
+    AL(child_alloc, uint8_t, NB);
+    AL(leaf, int, NB);
+    AL(lvl_leaf, int, NB);
+    AL(lvl_off, int, AMR_MAXLV + 1);
+    AL(freelist, int, (size_t)s.fl_cap);
+    AL(ref_list, int, NB);
+    AL(ref_c1, int, NB);
+    AL(der_list, int, NB);
+    AL(cnt, Counters, 1);
+    AL(queue, unsigned, 2 * NQUEUES);
+    ctx->d_diag = dalloc<double>(ctx, 9 + 9 * NB, &e);
+    if (e != cudaSuccess) {
+        int r = cuda_fail(ctx, e, "cudaMalloc diag");
+        amrlbm_destroy(ctx);
+        return r;
+    }
+#undef AL
+    ctx->lc.num_sms = sms;
+    ctx->lc.grid_queue = sms * 4;
+    ctx->lc.grid_leaves = sms * 4;
+    if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->t0) != cudaSuccess || cudaEventCreate(&ctx->t1) != cudaSuccess) {
+        amrlbm_destroy(ctx);
+        return AMRLBM_ERR_CUDA;
+    }
+    // 1 KB tile per block fits the default 48 KB dynamic shared memory
+    cudaDeviceSynchronize();
+    ctx->launches0 = launches_issued();
+    *out = ctx;
+    return AMRLBM_OK;
+}
+
+int amrlbm_destroy(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_OK;
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    for (auto& kv : ctx->graphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        for (auto& pe : kv.second.prof) {
+            cudaEventDestroy(pe.second.first);
+            cudaEventDestroy(pe.second.second);
+        }
+    }
+    for (void* p : ctx->allocs) cudaFree(p);
+    if (ctx->d_stage) cudaFree(ctx->d_stage);
+    if (ctx->d_ids) cudaFree(ctx->d_ids);
+    if (ctx->d_flush) cudaFree(ctx->d_flush);
+    if (ctx->t0) cudaEventDestroy(ctx->t0);
+    if (ctx->t1) cudaEventDestroy(ctx->t1);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+    return AMRLBM_OK;
+}
+
+int amrlbm_set_physics(amrlbm_ctx* ctx, const amrlbm_physics* phys) {
+    if (!ctx || !phys) return AMRLBM_ERR_ARG;
+    ctx->s.ph = to_physd(*phys);
+    for (auto& kv : ctx->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    ctx->graphs.clear();  // kernels capture DevState by value
+    return AMRLBM_OK;
+}
+
+const char* amrlbm_last_error(const amrlbm_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int64_t amrlbm_device_bytes(const amrlbm_ctx* ctx) { return ctx ? ctx->bytes : 0; }
+
+int amrlbm_get_counts(amrlbm_ctx* ctx, int32_t counts[5]) {
+    if (!ctx || !counts) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    Counters c = read_counters(ctx);
+    counts[0] = c.nblks;
+    counts[1] = c.nleaf;
+    counts[2] = c.kk;
+    counts[3] = c.level_min;
+    counts[4] = c.level_max;
+    return AMRLBM_OK;
+}
+
+int amrlbm_set_level_range(amrlbm_ctx* ctx, int32_t lmin, int32_t lmax) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    return set_level_counters(ctx, lmin, lmax);
+}
+
+int amrlbm_set_topology(amrlbm_ctx* ctx, int32_t nblks, const int32_t* level, const int32_t* dx,
+                        const int32_t* bi, const int32_t* bj, const int32_t* parent,
+                        const int32_t* child, const int32_t* nbr_owner, const int32_t* nbr_slot,
+                        const uint8_t* flags, int32_t n_free, const int32_t* free_list,
+                        int32_t kk) {
+    if (!ctx || nblks < 1 || nblks > ctx->prm.max_blks || n_free < 0 ||
+        n_free > ctx->s.fl_cap - 1 || !level || !dx || !bi || !bj || !parent || !child ||
+        !nbr_owner || !nbr_slot || !flags)
+        return AMRLBM_ERR_ARG;
+    DevState& s = ctx->s;
+    const size_t NB = (size_t)ctx->prm.max_blks + 1;
+    std::vector<int> lv(NB, -1), d(NB, 0), I(NB, 0), J(NB, 0), pa(NB, -1), ch(4 * NB, 0),
+        no(8 * NB, 0), ns(8 * NB, 0), zero8(8 * NB, 0), zero(NB, 0);
+    std::vector<uint8_t> fl[6];
+    for (auto& v : fl) v.assign(NB, 0);
+    for (int n = 1; n <= nblks; ++n) {
+        const int i = n - 1;
+        lv[n] = level[i];
+        d[n] = dx[i];
+        I[n] = bi[i];
+        J[n] = bj[i];
+        pa[n] = parent[i];
+        for (int k = 0; k < 4; ++k) ch[4 * n + k] = child[4 * i + k];
+        for (int k = 0; k < 8; ++k) {
+            no[8 * n + k] = nbr_owner[8 * i + k];
+            ns[8 * n + k] = nbr_slot[8 * i + k];
+            if (ns[8 * n + k] < 0 || ns[8 * n + k] > 4) return AMRLBM_ERR_ARG;
+            if (ns[8 * n + k] > 0 && (no[8 * n + k] < 1 || no[8 * n + k] > nblks))
+                return AMRLBM_ERR_ARG;
+        }
+        fl[0][n] = (flags[i] & AMRLBM_F_LEAF) ? 1 : 0;
+        fl[1][n] = (flags[i] & AMRLBM_F_HASLEAF) ? 1 : 0;
+        fl[2][n] = (flags[i] & AMRLBM_F_REFIN) ? 1 : 0;
+        fl[3][n] = (flags[i] & AMRLBM_F_DEREF) ? 1 : 0;
+        fl[4][n] = (flags[i] & AMRLBM_F_ALLOC) ? 1 : 0;
+        fl[5][n] = level[i] >= 0 ? 1 : 0;
+        if (level[i] >= AMR_MAXLV - 1) return AMRLBM_ERR_ARG;
+    }
+    for (int k = 0; k < n_free; ++k)
+        if (free_list[k] < 1 || free_list[k] + 3 > nblks) return AMRLBM_ERR_ARG;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->st);
+    };
+    CK(up(s.level, lv.data(), NB * 4));
+    CK(up(s.dx, d.data(), NB * 4));
+    CK(up(s.bi, I.data(), NB * 4));
+    CK(up(s.bj, J.data(), NB * 4));
+    CK(up(s.parent, pa.data(), NB * 4));
+    CK(up(s.child, ch.data(), 4 * NB * 4));
+    CK(up(s.nb_owner, no.data(), 8 * NB * 4));
+    CK(up(s.nb_slot, ns.data(), 8 * NB * 4));
+    CK(up(s.nb_gen, zero8.data(), 8 * NB * 4));
+    CK(up(s.gen, zero.data(), NB * 4));
+    CK(up(s.is_leaf, fl[0].data(), NB));
+    CK(up(s.has_leaf, fl[1].data(), NB));
+    CK(up(s.refin, fl[2].data(), NB));
+    CK(up(s.deref, fl[3].data(), NB));
+    CK(up(s.alloc, fl[4].data(), NB));
+    CK(up(s.child_alloc, fl[5].data(), NB));
+    if (n_free > 0) CK(up(s.freelist, free_list, (size_t)n_free * 4));
+    Counters c = read_counters(ctx);
+    c.nblks = nblks;
+    c.kk = kk;
+    c.fl_head = 0;
+    c.fl_count = n_free;
+    c.error = 0;
+    CK(cudaMemcpyAsync(s.cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, ctx->st));
+    launch_regrid_topo(s, ctx->st, 2, -1, -1, 0);
+    ctx->tail_done = true;
+    return sync_check(ctx);
+}
+
+int amrlbm_get_topology(amrlbm_ctx* ctx, int32_t* level, int32_t* dx, int32_t* bi, int32_t* bj,
+                        int32_t* parent, int32_t* child, int32_t* nbr_owner, int32_t* nbr_slot,
+                        uint8_t* flags, int32_t* n_free, int32_t* free_list) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    DevState& s = ctx->s;
+    Counters c = read_counters(ctx);
+    const size_t nb = (size_t)c.nblks + 1;
+    auto down = [&](std::vector<int>& v, const int* src, size_t n) {
+        v.resize(n);
+        return cudaMemcpy(v.data(), src, n * 4, cudaMemcpyDeviceToHost);
+    };
+    std::vector<int> lv, d, I, J, pa, ch, no, ns;
+    CK(down(lv, s.level, nb));
+    CK(down(d, s.dx, nb));
+    CK(down(I, s.bi, nb));
+    CK(down(J, s.bj, nb));
+    CK(down(pa, s.parent, nb));
+    CK(down(ch, s.child, 4 * nb));
+    CK(down(no, s.nb_owner, 8 * nb));
+    CK(down(ns, s.nb_slot, 8 * nb));
+    std::vector<uint8_t> fl[6];
+    const uint8_t* src[6] = {s.is_leaf, s.has_leaf, s.refin, s.deref, s.alloc, s.child_alloc};
+    for (int k = 0; k < 6; ++k) {
+        fl[k].resize(nb);
+        CK(cudaMemcpy(fl[k].data(), src[k], nb, cudaMemcpyDeviceToHost));
+    }
+    for (int n = 1; n <= c.nblks; ++n) {
+        const int i = n - 1;
+        if (level) level[i] = lv[n];
+        if (dx) dx[i] = d[n];
+        if (bi) bi[i] = I[n];
+        if (bj) bj[i] = J[n];
+        if (parent) parent[i] = pa[n];
+        if (child)
+            for (int k = 0; k < 4; ++k) child[4 * i + k] = fl[5][n] ? ch[4 * n + k] : 0;
+        for (int k = 0; k < 8; ++k) {
+            if (nbr_owner) nbr_owner[8 * i + k] = no[8 * n + k];
+            if (nbr_slot) nbr_slot[8 * i + k] = ns[8 * n + k];
+        }
+        if (flags)
+            flags[i] = (fl[0][n] ? AMRLBM_F_LEAF : 0) | (fl[1][n] ? AMRLBM_F_HASLEAF : 0) |
+                       (fl[2][n] ? AMRLBM_F_REFIN : 0) | (fl[3][n] ? AMRLBM_F_DEREF : 0) |
+                       (fl[4][n] ? AMRLBM_F_ALLOC : 0);
+    }
+    if (n_free) *n_free = c.fl_count;
+    if (free_list && c.fl_count > 0) {
+        std::vector<int> ring(s.fl_cap);
+        CK(cudaMemcpy(ring.data(), s.freelist, (size_t)s.fl_cap * 4, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < c.fl_count; ++k) free_list[k] = ring[(c.fl_head + k) % s.fl_cap];
+    }
+    return AMRLBM_OK;
+}
+
+int amrlbm_get_neighbours(amrlbm_ctx* ctx, int32_t* nbr) {
+    if (!ctx || !nbr) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    Counters c = read_counters(ctx);
+    const size_t nb = (size_t)c.nblks + 1;
+    std::vector<int> v(8 * nb);
+    std::vector<uint8_t> lf(nb);
+    CK(cudaMemcpy(v.data(), ctx->s.nbr, 8 * nb * 4, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(lf.data(), ctx->s.is_leaf, nb, cudaMemcpyDeviceToHost));
+    for (int n = 1; n <= c.nblks; ++n)
+        for (int k = 0; k < 8; ++k) nbr[8 * (n - 1) + k] = lf[n] ? v[8 * n + k] : 0;
+    return AMRLBM_OK;
+}
+
+int amrlbm_get_leaves(amrlbm_ctx* ctx, int32_t* leaves) {
+    if (!ctx || !leaves) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    Counters c = read_counters(ctx);
+    if (c.nleaf > 0)
+        CK(cudaMemcpy(leaves, ctx->s.leaf, (size_t)c.nleaf * 4, cudaMemcpyDeviceToHost));
+    return AMRLBM_OK;
+}
+
+int amrlbm_upload_fields(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, const double* h,
+                         const double* g, const double* C, const double* P, const double* Ux,
+                         const double* Uy) {
+    if (!ctx || n < 0 || (n > 0 && !ids)) return AMRLBM_ERR_ARG;
+    if (n == 0) return AMRLBM_OK;
+    int r = upload_blocks(ctx, n, ids, h, g, C, P, Ux, Uy);
+    if (r) return r;
+    ctx->tail_done = true;
+    return sync_check(ctx);
+}
+
+int amrlbm_download_fields(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, double* h, double* g,
+                           double* C, double* P, double* Ux, double* Uy) {
+    if (!ctx || n < 0 || (n > 0 && !ids)) return AMRLBM_ERR_ARG;
+    if (n == 0) return AMRLBM_OK;
+    for (int i = 0; i < n; ++i)
+        if (ids[i] < 1 || ids[i] > ctx->prm.max_blks) return AMRLBM_ERR_ARG;
+    if (int r = ensure_stage(ctx, (size_t)n)) return r;
+    const StageLayout L = stage_layout(ctx->prm.nx, ctx->prm.ny);
+    const int mask = (h ? 1 : 0) | (g ? 2 : 0) | (C ? 4 : 0) | (P ? 8 : 0) | (Ux ? 16 : 0) |
+                     (Uy ? 32 : 0);
+    CK(cudaMemcpyAsync(ctx->d_ids, ids, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->st));
+    k_transfer<<<ctx->lc.grid_leaves, 256, 0, ctx->st>>>(ctx->s, ctx->d_ids, n, ctx->d_stage, 1,
+                                                         mask, L);
+    CK(cudaGetLastError());
+    std::vector<double> host((size_t)n * L.per);
+    CK(cudaMemcpyAsync(host.data(), ctx->d_stage, host.size() * 8, cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    const size_t hs = L.g - L.h, cs = L.P - L.C, ps = L.Ux - L.P;
+    for (int i = 0; i < n; ++i) {
+        const double* rec = host.data() + (size_t)i * L.per;
+        if (h) std::memcpy(h + i * hs, rec + L.h, hs * 8);
+        if (g) std::memcpy(g + i * hs, rec + L.g, hs * 8);
+        if (C) std::memcpy(C + i * cs, rec + L.C, cs * 8);
+        if (P) std::memcpy(P + i * ps, rec + L.P, ps * 8);
+        if (Ux) std::memcpy(Ux + i * ps, rec + L.Ux, ps * 8);
+        if (Uy) std::memcpy(Uy + i * ps, rec + L.Uy, ps * 8);
+    }
+    return device_error(ctx);
+}
+
+int amrlbm_upload_block(amrlbm_ctx* ctx, int32_t id, const double* h, const double* g,
+                        const double* C, const double* P, const double* Ux, const double* Uy) {
+    return amrlbm_upload_fields(ctx, 1, &id, h, g, C, P, Ux, Uy);
+}
+
+int amrlbm_download_block(amrlbm_ctx* ctx, int32_t id, double* h, double* g, double* C,
+                          double* P, double* Ux, double* Uy) {
+    return amrlbm_download_fields(ctx, 1, &id, h, g, C, P, Ux, Uy);
+}
+
+int amrlbm_get_block_error(amrlbm_ctx* ctx, double* err) {
+    if (!ctx || !err) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    Counters c = read_counters(ctx);
+    std::vector<double> e((size_t)c.nblks + 1);
+    std::vector<uint8_t> lf((size_t)c.nblks + 1);
+    CK(cudaMemcpy(e.data(), ctx->s.err, e.size() * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(lf.data(), ctx->s.is_leaf, lf.size(), cudaMemcpyDeviceToHost));
+    for (int n = 1; n <= c.nblks; ++n) err[n - 1] = lf[n] ? e[n] : 0.0;
+    return AMRLBM_OK;
+}
+
+// Initialize_AMR_Rising_Bubble (AMR_Rising_2D_OMP.f90:142-231): the analytic
+// C (tanh profile, both ghost rings) is evaluated on the host like the
+// driver does; P, U, h and g are derived from it on the device.
+int amrlbm_init_fields(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    std::vector<int> leaves;
+    HostTopo t;
+    if (int r = get_leaves_host(ctx, leaves, t)) return r;
+    const int nx = ctx->prm.nx, ny = ctx->prm.ny;
+    const double R = ctx->prm.radius, X0 = ctx->prm.xc, Y0 = ctx->prm.yc, W = ctx->s.ph.W;
+    const size_t cs = (size_t)(nx + 4) * (ny + 4);
+    std::vector<double> C(leaves.size() * cs);
+    for (size_t m = 0; m < leaves.size(); ++m) {
+        const int n = leaves[m];
+        const int dx = t.dx[n];
+        double* c = C.data() + m * cs;
+        for (int j = -1; j <= ny + 2; ++j)
+            for (int i = -1; i <= nx + 2; ++i) {
+                const double Xc = (double)(t.bi[n] * dx * nx) + dx * (i - 0.5);
+                const double Yc = (double)(t.bj[n] * dx * ny) + dx * (j - 0.5);
+                const double Ri = std::sqrt((Xc - X0) * (Xc - X0) + (Yc - Y0) * (Yc - Y0));
+                c[(i + 1) + (nx + 4) * (j + 1)] = 0.5 + 0.5 * std::tanh(2.0 * (Ri - R) / W);
+            }
+    }
+    if (!leaves.empty()) {
+        if (int r = upload_blocks(ctx, (int)leaves.size(), leaves.data(), nullptr, nullptr,
+                                  C.data(), nullptr, nullptr, nullptr))
+            return r;
+    }
+    launch_init_fields(ctx->s, ctx->lc, ctx->st, R);
+    ctx->tail_done = true;
+    return sync_check(ctx);
+}
+
+// AMR_LBM_Rising_Bubble (AMR_Rising_2D_OMP.f90:49-67) with the base grid
+// generalised to nbx x nby blocks (periodic in x, walls in y).
+int amrlbm_init_rising_bubble(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    const amrlbm_params& p = ctx->prm;
+    const int nbx = p.nbx, nby = p.nby, nb = nbx * nby;
+    // Initialize_Base_Block + Fix_Initial_Neighbors_3Blocks (:79-138)
+    std::vector<int> level(nb, 0), dx(nb, p.dx0), bi(nb), bj(nb), parent(nb, -1), child(4 * nb),
+        own(8 * nb), slot(8 * nb, 0);
+    std::vector<uint8_t> flags(nb, AMRLBM_F_LEAF | (p.min_levels == 0 ? AMRLBM_F_ALLOC : 0));
+    auto id = [&](int x, int y) { return 1 + ((x % nbx + nbx) % nbx) + nbx * y; };
+    for (int y = 0; y < nby; ++y)
+        for (int x = 0; x < nbx; ++x) {
+            const int n = id(x, y), i = n - 1;
+            bi[i] = x;
+            bj[i] = y;
+            for (int k = 0; k < 4; ++k) child[4 * i + k] = n;  // child(:) = self (see DESIGN)
+            const bool lo = y > 0, hi = y < nby - 1;
+            const int v[8] = {id(x - 1, y),
+                              id(x + 1, y),
+                              lo ? id(x, y - 1) : -3,
+                              hi ? id(x, y + 1) : -4,
+                              lo ? id(x - 1, y - 1) : -5,
+                              hi ? id(x - 1, y + 1) : -6,
+                              lo ? id(x + 1, y - 1) : -7,
+                              hi ? id(x + 1, y + 1) : -8};
+            for (int k = 0; k < 8; ++k) own[8 * i + k] = v[k];
+        }
+    if (int r = amrlbm_set_topology(ctx, nb, level.data(), dx.data(), bi.data(), bj.data(),
+                                    parent.data(), child.data(), own.data(), slot.data(),
+                                    flags.data(), 0, nullptr, 0))
+        return r;
+    // zero the base blocks' fields
+    {
+        std::vector<int> ids(nb);
+        for (int n = 1; n <= nb; ++n) ids[n - 1] = n;
+        const StageLayout L = stage_layout(p.nx, p.ny);
+        std::vector<double> z((size_t)nb * (L.per));
+        const size_t hs = L.g - L.h, cs = L.P - L.C, ps = L.Ux - L.P;
+        std::vector<double> zh(nb * hs, 0.0), zc(nb * cs, 0.0), zp(nb * ps, 0.0);
+        if (int r = upload_blocks(ctx, nb, ids.data(), zh.data(), zh.data(), zc.data(), zp.data(),
+                                  zp.data(), zp.data()))
+            return r;
+    }
+    // Initial_Mesh (:493-513)
+    for (int L = 1; L <= p.min_levels; ++L) {
+        launch_flag_level(ctx->s, ctx->st, L - 1);
+        launch_regrid_topo(ctx->s, ctx->st, 1, L - 1, L - 1, 0);
+        launch_zero_children(ctx->s, ctx->lc, ctx->st);
+    }
+    if (int r = sync_check(ctx)) return r;
+    int lmin = p.min_levels, lmax = p.min_levels;
+    if (int r = set_level_counters(ctx, lmin, lmax)) return r;
+    if (int r = amrlbm_init_fields(ctx)) return r;
+    while (lmax < p.max_levels) {
+        if (int r = amrlbm_regrid(ctx, p.refin_tol, p.deref_tol)) return r;
+        if (int r = amrlbm_init_fields(ctx)) return r;
+        lmax = lmax + 1;
+        if (int r = set_level_counters(ctx, lmin, lmax)) return r;
+    }
+    ctx->stepcount = 0;
+    ctx->tail_done = true;
+    return AMRLBM_OK;
+}
+
+int amrlbm_min_max_levels(amrlbm_ctx* ctx, int32_t* lmin, int32_t* lmax) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    launch_minmax(ctx->s, ctx->st);
+    if (int r = sync_check(ctx)) return r;
+    Counters c = read_counters(ctx);
+    if (lmin) *lmin = c.level_min;
+    if (lmax) *lmax = c.level_max;
+    return AMRLBM_OK;
+}
+
+int amrlbm_fill_ghost_c2(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    launch_fill_c(ctx->s, ctx->lc, ctx->st, 2, CONS_NONE);
+    return sync_check(ctx);
+}
+
+int amrlbm_phase_field_step(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    launch_collide(ctx->s, ctx->lc, ctx->st);
+    launch_fill_hg_stream(ctx->s, ctx->lc, ctx->st);
+    ctx->tail_done = false;
+    return sync_check(ctx);
+}
+
+int amrlbm_macro_h(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    launch_macro_h(ctx->s, ctx->lc, ctx->st);
+    return sync_check(ctx);
+}
+
+int amrlbm_fill_ghost_c(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    launch_fill_c(ctx->s, ctx->lc, ctx->st, 1, CONS_NONE);
+    return sync_check(ctx);
+}
+
+int amrlbm_macro_g(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    launch_macro_g(ctx->s, ctx->lc, ctx->st);
+    ctx->tail_done = true;
+    return sync_check(ctx);
+}
+
+int amrlbm_regrid(amrlbm_ctx* ctx, double refin_tol, double deref_tol) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    enqueue_regrid(ctx, refin_tol, deref_tol, true, false);
+    ctx->tail_done = true;
+    return sync_check(ctx);
+}
+
+int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
+    if (!ctx || nsteps < 0) return AMRLBM_ERR_ARG;
+    if (nsteps == 0) return AMRLBM_OK;
+    const int R = ctx->prm.regrid_every;
+    launch_minmax(ctx->s, ctx->st);  // Determine_Min_Max_Levels
+    int done = 0;
+    while (done < nsteps) {
+        const int phase = (int)(ctx->stepcount % R);
+        int chunk = (R == 1) ? 16 : R - phase;  // up to the next regrid
+        if (chunk > nsteps - done) chunk = nsteps - done;
+        const bool final_chunk = (done + chunk == nsteps);
+        const auto key = std::make_tuple(chunk, phase, ctx->tail_done ? 1 : 0, final_chunk ? 1 : 0,
+                                         ctx->prof ? 1 : 0);
+        auto it = ctx->graphs.find(key);
+        if (it == ctx->graphs.end()) {
+            GraphEntry ge;
+            CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+            bool prev_tail = ctx->tail_done;
+            for (int t = 0; t < chunk; ++t) {
+                const bool regrid = ((phase + t + 1) % R) == 0;
+                const bool tail = regrid || (final_chunk && t == chunk - 1);
+                enqueue_step(ctx, &ge, prev_tail, tail, regrid);
+                prev_tail = tail;
+            }
+            cudaGraph_t g;
+            CK(cudaStreamEndCapture(ctx->st, &g));
+            CK(cudaGraphInstantiate(&ge.exec, g, 0));
+            cudaGraphDestroy(g);
+            it = ctx->graphs.emplace(key, ge).first;
+        }
+        CK(cudaGraphLaunch(it->second.exec, ctx->st));
+        // regrid / tail state after the chunk
+        bool last_tail = false;
+        for (int t = 0; t < chunk; ++t) {
+            const bool regrid = ((phase + t + 1) % R) == 0;
+            last_tail = regrid || (final_chunk && t == chunk - 1);
+        }
+        if (ctx->prof) {
+            CK(cudaStreamSynchronize(ctx->st));
+            for (auto& pe : it->second.prof) {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, pe.second.first, pe.second.second);
+                ctx->prof_ms[pe.first] += ms;
+                ctx->prof_n[pe.first] += 1;
+            }
+        }
+        ctx->stepcount += chunk;
+        ctx->tail_done = last_tail;
+        done += chunk;
+    }
+    CK(cudaGetLastError());
+    return AMRLBM_OK;
+}
+
+int amrlbm_sync(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    return sync_check(ctx);
+}
+
+int amrlbm_diag(amrlbm_ctx* ctx, double out[8]) {
+    if (!ctx || !out) return AMRLBM_ERR_ARG;
+    launch_diag(ctx->s, ctx->st, ctx->d_diag);
+    double o[9];
+    CK(cudaMemcpyAsync(o, ctx->d_diag, 9 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    if (int r = sync_check(ctx)) return r;
+    for (int k = 0; k < 8; ++k) out[k] = o[k];
+    if (o[8] != 0.0) return fail(ctx, AMRLBM_ERR_NAN, "non-finite C or Uy in a leaf");
+    return AMRLBM_OK;
+}
+
+int amrlbm_timer_start(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    CK(cudaEventRecord(ctx->t0, ctx->st));
+    return AMRLBM_OK;
+}
+
+int amrlbm_timer_stop(amrlbm_ctx* ctx, float* ms) {
+    if (!ctx || !ms) return AMRLBM_ERR_ARG;
+    CK(cudaEventRecord(ctx->t1, ctx->st));
+    CK(cudaEventSynchronize(ctx->t1));
+    CK(cudaEventElapsedTime(ms, ctx->t0, ctx->t1));
+    return device_error(ctx);
+}
+
+int amrlbm_profile_enable(amrlbm_ctx* ctx, int32_t enable) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    ctx->prof = enable != 0;
+    for (int k = 0; k < 4; ++k) {
+        ctx->prof_ms[k] = 0;
+        ctx->prof_n[k] = 0;
+    }
+    return AMRLBM_OK;
+}
+
+int amrlbm_profile_read(amrlbm_ctx* ctx, int32_t kernel, double* total_ms, int64_t* launches,
+                        int64_t* cells) {
+    if (!ctx || kernel < 0 || kernel > 3) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    if (total_ms) *total_ms = ctx->prof_ms[kernel];
+    if (launches) *launches = ctx->prof_n[kernel];
+    if (cells) {
+        Counters c = read_counters(ctx);
+        *cells = (int64_t)c.updates;
+    }
+    return AMRLBM_OK;
+}
+
+int64_t amrlbm_launch_count(const amrlbm_ctx* ctx) {
+    return ctx ? (int64_t)(launches_issued() - ctx->launches0) : 0;
+}
+
+int amrlbm_flush_l2(amrlbm_ctx* ctx) {
+    if (!ctx) return AMRLBM_ERR_ARG;
+    if (!ctx->d_flush) {
+        int dev = 0, l2 = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+        ctx->flush_bytes = (size_t)(l2 > 0 ? l2 : (126 << 20)) * 2;
+        CK(cudaMalloc(&ctx->d_flush, ctx->flush_bytes));
+    }
+    CK(cudaMemsetAsync(ctx->d_flush, ctx->flush_bytes & 0xff, ctx->flush_bytes, ctx->st));
+    return AMRLBM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+int upload_blocks(amrlbm_ctx* ctx, int n, const int* ids, const double* h, const double* g,
+                  const double* C, const double* P, const double* Ux, const double* Uy) {
+    for (int i = 0; i < n; ++i)
+        if (ids[i] < 1 || ids[i] > ctx->prm.max_blks) return AMRLBM_ERR_ARG;
+    if (int r = ensure_stage(ctx, (size_t)n)) return r;
+    const StageLayout L = stage_layout(ctx->prm.nx, ctx->prm.ny);
+    const int mask = (h ? 1 : 0) | (g ? 2 : 0) | (C ? 4 : 0) | (P ? 8 : 0) | (Ux ? 16 : 0) |
+                     (Uy ? 32 : 0);
+    std::vector<double> host((size_t)n * L.per, 0.0);
+    const size_t hs = L.g - L.h, cs = L.P - L.C, ps = L.Ux - L.P;
+    for (int i = 0; i < n; ++i) {
+        double* rec = host.data() + (size_t)i * L.per;
+        if (h) std::memcpy(rec + L.h, h + i * hs, hs * 8);
+        if (g) std::memcpy(rec + L.g, g + i * hs, hs * 8);
+        if (C) std::memcpy(rec + L.C, C + i * cs, cs * 8);
+        if (P) std::memcpy(rec + L.P, P + i * ps, ps * 8);
+        if (Ux) std::memcpy(rec + L.Ux, Ux + i * ps, ps * 8);
+        if (Uy) std::memcpy(rec + L.Uy, Uy + i * ps, ps * 8);
+    }
+    CK(cudaMemcpyAsync(ctx->d_stage, host.data(), host.size() * 8, cudaMemcpyHostToDevice,
+                       ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_ids, ids, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->st));
+    k_transfer<<<ctx->lc.grid_leaves, 256, 0, ctx->st>>>(ctx->s, ctx->d_ids, n, ctx->d_stage, 0,
+                                                         mask, L);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));  // host buffer goes out of scope
+    return 0;
+}
+}  // namespace

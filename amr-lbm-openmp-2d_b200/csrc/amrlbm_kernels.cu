@@ -1,0 +1,1291 @@
+// amrlbm_kernels.cu - FP64 sm_100a kernels of the block-structured AMR
+// two-phase lattice Boltzmann step. Compiled with -fmad=false: every FP64
+// operation is rounded separately, in the reference's order.
+//
+// Level-ordered launches. The reference fills ghost cells level by level
+// (Fill_Ghost_Cells_C.f90:8-38): a coarse-to-fine fill reads the coarse
+// neighbour's ghost ring, which the previous level wrote. Here one launch
+// serves all levels: CTAs claim leaves from a queue sorted by level; a leaf
+// of level L waits (bounded spin) until every leaf of a coarser level has
+// published its ring. A waited-on leaf was claimed earlier by a running CTA,
+// so the wait always ends. After its fill a CTA goes on with the work that
+// only needs its own ring (collision, streaming, macroscopic values), so one
+// launch does "fill + consumer" with no grid-wide barrier.
+#include <cstdio>
+
+#include "amrlbm_launch.h"
+
+namespace {
+
+long long g_launches = 0;
+
+constexpr int kSpinLimit = 20000000;  // x ~64 ns: about a second
+
+__device__ __forceinline__ int ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return (int)v;
+}
+
+// Claims the next item of queue q; returns its index (block-uniform).
+__device__ __forceinline__ int claim(const DevState& s, int q, int* slot) {
+    __syncthreads();
+    if (threadIdx.x == 0) *slot = (int)atomicAdd(&s.queue[2 * q], 1u);
+    __syncthreads();
+    return *slot;
+}
+
+// Waits until `target` items of queue q are done (thread 0 spins).
+__device__ __forceinline__ void wait_done(const DevState& s, int q, int target) {
+    if (threadIdx.x == 0 && target > 0) {
+        int it = 0;
+        while (ld_acquire(&s.queue[2 * q + 1]) < target) {
+            if (++it > kSpinLimit) {
+                set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, q);
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void publish_done(const DevState& s, int q) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&s.queue[2 * q + 1], 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fill_Ghost_Cells_C / _C2: value of ghost cell (x,y) of block n (level L)
+// from its direction-d neighbour N. Returns 1 if written, -1 on a level jump.
+// The gathers and stencils mirror Fill_Left_C .. Fill_Right_Top_C
+// (Fill_Ghost_Cells_C.f90:44-416, _C2.f90:44-416) case by case.
+__device__ int fill_c_value(const DevState& s, int n, int L, int N, int d, int x, int y,
+                            double& v) {
+    const int nx = s.nx, ny = s.ny;
+    const int Ln = s.level[N];
+    const bool left = (d == 1 || d == 5 || d == 6), right = (d == 2 || d == 7 || d == 8);
+    const bool bottom = (d == 3 || d == 5 || d == 7), top = (d == 4 || d == 6 || d == 8);
+    const int a = left ? 1 - x : (right ? x - nx : 0);  // layer counted outward
+    const int b = bottom ? 1 - y : (top ? y - ny : 0);
+    const double* C = s.C;
+    if (L == Ln) {
+        if (s.is_leaf[N]) {  // same-level leaf: copy
+            const int sx = left ? nx + 1 - a : (right ? a : x);
+            const int sy = bottom ? ny + 1 - b : (top ? b : y);
+            v = ldcg(&C[c_idx(s, N, sx, sy)]);
+            return 1;
+        }
+        const int c1 = s.child[4 * N];  // same-level parent: Biquadratic_from_Fine
+        if (d == 1 || d == 2) {
+            v = biq_fine_pt(a, y, [&](int r, int J) {
+                const int ch = (J <= ny) ? (d == 1 ? c1 + 1 : c1) : (d == 1 ? c1 + 3 : c1 + 2);
+                const int jj = (J <= ny) ? J : J - ny;
+                const int xx = (d == 1) ? nx - r + 1 : r;
+                return ldcg(&C[c_idx(s, ch, xx, jj)]);
+            });
+        } else if (d == 3 || d == 4) {
+            v = biq_fine_pt(x, b, [&](int I, int r) {
+                const int ch = (I <= nx) ? (d == 3 ? c1 + 2 : c1) : (d == 3 ? c1 + 3 : c1 + 1);
+                const int ii = (I <= nx) ? I : I - nx;
+                const int yy = (d == 3) ? ny - r + 1 : r;
+                return ldcg(&C[c_idx(s, ch, ii, yy)]);
+            });
+        } else {
+            const int ch = c1 + (d == 5 ? 3 : d == 6 ? 1 : d == 7 ? 2 : 0);
+            v = biq_fine_pt(a, b, [&](int k, int l) {
+                const int xx = left ? nx - k + 1 : k;
+                const int yy = bottom ? ny - l + 1 : l;
+                return ldcg(&C[c_idx(s, ch, xx, yy)]);
+            });
+        }
+        return 1;
+    }
+    if (L == Ln + 1) {  // coarser neighbour: Biquadratic_from_Coarse
+        if (d == 1 || d == 2) {
+            const int Y = (ny / 2) * (s.bj[n] % 2);
+            v = biq_coarse_pt(a, y, [&](int ii, int jj) {
+                const int xx = (d == 1) ? nx + 2 - ii : ii - 1;
+                return ldcg(&C[c_idx(s, N, xx, jj - 1 + Y)]);
+            });
+        } else if (d == 3 || d == 4) {
+            const int X = (nx / 2) * (s.bi[n] % 2);
+            v = biq_coarse_pt(x, b, [&](int ii, int jj) {
+                const int yy = (d == 3) ? ny + 2 - jj : jj - 1;
+                return ldcg(&C[c_idx(s, N, ii - 1 + X, yy)]);
+            });
+        } else {
+            const int mi = s.bi[n] % 2, mj = s.bj[n] % 2;
+            const int I = left ? nx - (nx / 2) * mi - 1 : nx / 2 - (nx / 2) * mi;
+            const int J = bottom ? ny - (ny / 2) * mj - 1 : ny / 2 - (ny / 2) * mj;
+            v = biq_coarse_pt(a, b, [&](int ii, int jj) {
+                const int xx = left ? I + 3 - ii : I + ii - 1;
+                const int yy = bottom ? J + 3 - jj : J + jj - 1;
+                return ldcg(&C[c_idx(s, N, xx, yy)]);
+            });
+        }
+        return 1;
+    }
+    return -1;
+}
+
+// direction (1..8) of ghost cell (x,y)
+__device__ __forceinline__ int ghost_dir(int x, int y, int nx, int ny) {
+    const bool xl = x < 1, xr = x > nx, yb = y < 1, yt = y > ny;
+    if (xl) return yb ? 5 : (yt ? 6 : 1);
+    if (xr) return yb ? 7 : (yt ? 8 : 2);
+    return yb ? 3 : 4;
+}
+
+// Fills the C ring of width w of block n into global memory and into the
+// shared tile T ((nx+4) x (ny+4), index (y+2)*(nx+4)+(x+2)); the interior of
+// T must already be loaded. Ends with the ring complete in T and in memory.
+__device__ void fill_c_block(const DevState& s, int n, int L, const int* nb, int w,
+                             double* T) {
+    const int nx = s.nx, ny = s.ny, TW = nx + 4;
+    const int W = nx + 2 * w, H = ny + 2 * w;
+    for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x) {
+        const int x = idx % W - w + 1, y = idx / W - w + 1;
+        if (x >= 1 && x <= nx && y >= 1 && y <= ny) continue;
+        const int d = ghost_dir(x, y, nx, ny);
+        const int N = nb[d];
+        if (N <= 0) continue;
+        double v;
+        const int r = fill_c_value(s, n, L, N, d, x, y, v);
+        if (r < 0) {
+            set_error(s, 4 /*AMRLBM_ERR_LEVEL_JUMP*/, n);
+            continue;
+        }
+        s.C[c_idx(s, n, x, y)] = v;
+        T[(y + 2) * TW + (x + 2)] = v;
+    }
+    __syncthreads();
+    // Symmetric_C(2)_3/4 (BC_Cell.f90:46-104): overwrite the wall rows
+    if (nb[3] < 0) {
+        for (int X = threadIdx.x - (w - 1); X <= nx + w; X += blockDim.x) {
+            if (X < 1 - w) continue;
+            for (int a = 1; a <= w; ++a) {  // C(X,1-a) = C(X,a)
+                const double v = T[(a + 2) * TW + (X + 2)];
+                T[(1 - a + 2) * TW + (X + 2)] = v;
+                s.C[c_idx(s, n, X, 1 - a)] = v;
+            }
+        }
+    }
+    if (nb[4] < 0) {
+        for (int X = threadIdx.x - (w - 1); X <= nx + w; X += blockDim.x) {
+            if (X < 1 - w) continue;
+            for (int a = 1; a <= w; ++a) {  // C(X,ny+a) = C(X,ny+1-a)
+                const double v = T[(ny + 1 - a + 2) * TW + (X + 2)];
+                T[(ny + a + 2) * TW + (X + 2)] = v;
+                s.C[c_idx(s, n, X, ny + a)] = v;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Fill_Ghost_Cells_hg (Fill_Ghost_Cells_hg.f90:53-477): ghost cell (x,y) of
+// population q of the post-collision field A.
+__device__ int fill_hg_value(const DevState& s, const double* A, int n, int L, int N, int d,
+                             int q, int x, int y, double& v) {
+    const int nx = s.nx, ny = s.ny;
+    const int Ln = s.level[N];
+    const bool left = (d == 1 || d == 5 || d == 6), right = (d == 2 || d == 7 || d == 8);
+    const bool bottom = (d == 3 || d == 5 || d == 7), top = (d == 4 || d == 6 || d == 8);
+    if (L == Ln) {
+        if (s.is_leaf[N]) {
+            const int sx = left ? nx : (right ? 1 : x);
+            const int sy = bottom ? ny : (top ? 1 : y);
+            v = ldcg(&A[a_idx(s, N, q, sx, sy)]);
+            return 1;
+        }
+        const int c1 = s.child[4 * N];
+        if (d == 1 || d == 2) {
+            v = biq_fine_pt(1, y, [&](int r, int J) {
+                const int ch = (J <= ny) ? (d == 1 ? c1 + 1 : c1) : (d == 1 ? c1 + 3 : c1 + 2);
+                const int jj = (J <= ny) ? J : J - ny;
+                const int xx = (d == 1) ? nx - r + 1 : r;
+                return ldcg(&A[a_idx(s, ch, q, xx, jj)]);
+            });
+        } else if (d == 3 || d == 4) {
+            v = biq_fine_pt(x, 1, [&](int I, int r) {
+                const int ch = (I <= nx) ? (d == 3 ? c1 + 2 : c1) : (d == 3 ? c1 + 3 : c1 + 1);
+                const int ii = (I <= nx) ? I : I - nx;
+                const int yy = (d == 3) ? ny - r + 1 : r;
+                return ldcg(&A[a_idx(s, ch, q, ii, yy)]);
+            });
+        } else {
+            const int ch = c1 + (d == 5 ? 3 : d == 6 ? 1 : d == 7 ? 2 : 0);
+            v = biq_fine_pt(1, 1, [&](int k, int l) {
+                const int xx = left ? nx - k + 1 : k;
+                const int yy = bottom ? ny - l + 1 : l;
+                return ldcg(&A[a_idx(s, ch, q, xx, yy)]);
+            });
+        }
+        return 1;
+    }
+    if (L == Ln + 1) {
+        if (d == 1 || d == 2) {
+            const int Y = (ny / 2) * (s.bj[n] % 2);
+            v = biq_coarse_pt(1, y, [&](int ii, int jj) {
+                const int xx = (d == 1) ? nx + 2 - ii : ii - 1;
+                return ldcg(&A[a_idx(s, N, q, xx, jj - 1 + Y)]);
+            });
+        } else if (d == 3 || d == 4) {
+            const int X = (nx / 2) * (s.bi[n] % 2);
+            v = biq_coarse_pt(x, 1, [&](int ii, int jj) {
+                const int yy = (d == 3) ? ny + 2 - jj : jj - 1;
+                return ldcg(&A[a_idx(s, N, q, ii - 1 + X, yy)]);
+            });
+        } else {
+            const int mi = s.bi[n] % 2, mj = s.bj[n] % 2;
+            const int I = left ? nx - (nx / 2) * mi - 1 : nx / 2 - (nx / 2) * mi;
+            const int J = bottom ? ny - (ny / 2) * mj - 1 : ny / 2 - (ny / 2) * mj;
+            v = biq_coarse_pt(1, 1, [&](int ii, int jj) {
+                const int xx = left ? I + 3 - ii : I + ii - 1;
+                const int yy = bottom ? J + 3 - jj : J + jj - 1;
+                return ldcg(&A[a_idx(s, N, q, xx, yy)]);
+            });
+        }
+        return 1;
+    }
+    return -1;
+}
+
+// ring cell index r in [0, 2(nx+ny)+4) -> (x,y) of ring 1
+__device__ __forceinline__ void ring1_xy(int r, int nx, int ny, int& x, int& y) {
+    if (r < nx + 2) {
+        x = r;
+        y = 0;
+    } else if (r < 2 * (nx + 2)) {
+        x = r - (nx + 2);
+        y = ny + 1;
+    } else {
+        const int t = r - 2 * (nx + 2);
+        x = (t < ny) ? 0 : nx + 1;
+        y = 1 + (t < ny ? t : t - ny);
+    }
+}
+
+// Fills ring 1 of h and g (post-collision A arrays) of block n, then applies
+// Bounce_Back_3/4 (BC_Cell.f90:2-42).
+__device__ void fill_hg_block(const DevState& s, int n, int L, const int* nb) {
+    const int nx = s.nx, ny = s.ny;
+    const int R = 2 * (nx + ny) + 4;
+    for (int idx = threadIdx.x; idx < R * 18; idx += blockDim.x) {
+        const int r = idx % R, qf = idx / R;
+        const int q = qf % 9 + 1;
+        double* A = (qf < 9) ? s.Ah : s.Ag;
+        int x, y;
+        ring1_xy(r, nx, ny, x, y);
+        const int d = ghost_dir(x, y, nx, ny);
+        const int N = nb[d];
+        if (N <= 0) continue;
+        double v;
+        if (fill_hg_value(s, A, n, L, N, d, q, x, y, v) < 0) {
+            set_error(s, 4, n);
+            continue;
+        }
+        A[a_idx(s, n, q, x, y)] = v;
+    }
+    __syncthreads();
+    for (int wall = 3; wall <= 4; ++wall) {
+        if (nb[wall] >= 0) continue;
+        const int Y = (wall == 3) ? 0 : ny + 1, Yi = (wall == 3) ? 1 : ny;
+        const int sgn = (wall == 3) ? 1 : -1;
+        for (int idx = threadIdx.x; idx < (nx + 2) * 18; idx += blockDim.x) {
+            const int X = idx % (nx + 2), qf = idx / (nx + 2);
+            const int i = qf % 9 + 1;
+            double* A = (qf < 9) ? s.Ah : s.Ag;
+            double v;
+            if (i == 1) {
+                v = A[a_idx(s, n, 1, X, Yi)];
+            } else {
+                int Xn = X + sgn * d_ex[i] * d_ey[i];
+                Xn = min(max(0, Xn), nx + 1);
+                const int J = (i - 2) + 4 * ((i / 2) % 2);
+                v = A[a_idx(s, n, J, Xn, Yi)];
+            }
+            A[a_idx(s, n, i, X, Y)] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// collision of one cell of block n from the shared C tile T
+template <int CONSUMER>
+__device__ __forceinline__ void collide_consumer(const DevState& s, int n, const double* T) {
+    const int nx = s.nx, ny = s.ny, TW = nx + 4;
+    const int dx = s.dx[n];
+    for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+        const int x = c % nx + 1, y = c / nx + 1;
+        auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 2) * TW + (x + ddx + 2)]; };
+        double h[10], g[10];
+#pragma unroll
+        for (int q = 1; q <= 9; ++q) {
+            h[q] = s.Bh[b_idx(s, n, q, x, y)];
+            g[q] = s.Bg[b_idx(s, n, q, x, y)];
+        }
+        double P, Ux, Uy;
+        if (CONSUMER == CONS_COLLIDE_FUSED) {
+            macro_g_cell(s.ph, dx, Cs, g, P, Ux, Uy);
+        } else {
+            P = s.P[p_idx(s, n, x, y)];
+            Ux = s.Ux[p_idx(s, n, x, y)];
+            Uy = s.Uy[p_idx(s, n, x, y)];
+        }
+        collide_cell(s.ph, dx, Cs, P, Ux, Uy, h, g);
+#pragma unroll
+        for (int q = 1; q <= 9; ++q) {
+            s.Ah[a_idx(s, n, q, x, y)] = h[q];
+            s.Ag[a_idx(s, n, q, x, y)] = g[q];
+        }
+    }
+}
+
+// Macroscopic_Values_g_AMR + Err_Interface of block n from the tile T
+__device__ void macro_g_err_consumer(const DevState& s, int n, const double* T, double* red) {
+    const int nx = s.nx, ny = s.ny, TW = nx + 4;
+    const int dx = s.dx[n];
+    double mx = 0.0;
+    for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+        const int x = c % nx + 1, y = c / nx + 1;
+        auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 2) * TW + (x + ddx + 2)]; };
+        double g[10];
+#pragma unroll
+        for (int q = 1; q <= 9; ++q) g[q] = s.Bg[b_idx(s, n, q, x, y)];
+        double P, Ux, Uy;
+        macro_g_cell(s.ph, dx, Cs, g, P, Ux, Uy);
+        s.P[p_idx(s, n, x, y)] = P;
+        s.Ux[p_idx(s, n, x, y)] = Ux;
+        s.Uy[p_idx(s, n, x, y)] = Uy;
+        const double a = Cs(1, 0) - Cs(-1, 0), b = Cs(0, 1) - Cs(0, -1);
+        mx = fmax(mx, a * a + b * b);
+    }
+    // block max; fmax drops NaN like MAX(err, DC) with a NaN DC never chosen
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) m = fmax(m, red[w]);
+        s.err[n] = sqrt(m) / (2.0 * dx);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Level-ordered C ghost fill (+ consumer). Items: all leaves grouped by
+// level; leaves of levels outside [LevelMin, LevelMax] are not filled (as the
+// reference's DO L = LevelMin, LevelMax) but still get the consumer work.
+template <int CONSUMER>
+__global__ void __launch_bounds__(256) k_fill_c(DevState s, int w, int q) {
+    extern __shared__ double sm[];
+    double* T = sm;
+    double* red = sm + (s.nx + 4) * (s.ny + 4);
+    __shared__ int s_item, s_nb[9];
+    const int nx = s.nx, ny = s.ny, TW = nx + 4;
+    const int lmin = s.cnt->level_min, lmax = s.cnt->level_max;
+    const int total = s.lvl_off[AMR_MAXLV];
+    if (CONSUMER == CONS_COLLIDE_READ || CONSUMER == CONS_COLLIDE_FUSED)
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            atomicAdd(&s.cnt->updates, (unsigned long long)total * (unsigned long long)(nx * ny));
+    for (;;) {
+        const int k = claim(s, q, &s_item);
+        if (k >= total) break;
+        const int n = s.lvl_leaf[k];
+        const int L = s.level[n];
+        if (threadIdx.x < 8) s_nb[threadIdx.x + 1] = s.nbr[8 * n + threadIdx.x];
+        // the whole tile from memory; the fill overwrites the ring cells it owns
+        {
+            const int W = nx + 4, H = ny + 4;
+            for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x)
+                T[idx] = ldcg(&s.C[c_idx(s, n, idx % W - 2, idx / W - 2)]);
+        }
+        const bool do_fill = (L >= lmin && L <= lmax);
+        if (do_fill) {
+            wait_done(s, q, (L > 0) ? s.lvl_off[L] : 0);
+            fill_c_block(s, n, L, s_nb, w, T);
+        } else {
+            __syncthreads();
+        }
+        publish_done(s, q);
+        if (CONSUMER != CONS_NONE) {
+            __syncthreads();
+            if (CONSUMER == CONS_MACRO_G)
+                macro_g_err_consumer(s, n, T, red);
+            else
+                collide_consumer<CONSUMER>(s, n, T);
+        }
+    }
+    (void)TW;
+}
+
+// Level-ordered Fill_Ghost_Cells_hg + streaming (Perfect_Shift_AMR or
+// Streaming_LaxWendroff_AMR, LBM_Subroutines.f90:41-90) from A into B +
+// Macroscopic_Values_h_AMR (:193-201).
+__global__ void __launch_bounds__(256) k_fill_hg_stream(DevState s) {
+    __shared__ int s_item, s_nb[9];
+    const int nx = s.nx, ny = s.ny;
+    const int q = Q_FILLHG;
+    const int lmin = s.cnt->level_min, lmax = s.cnt->level_max;
+    const int total = s.lvl_off[AMR_MAXLV];
+    for (;;) {
+        const int k = claim(s, q, &s_item);
+        if (k >= total) break;
+        const int n = s.lvl_leaf[k];
+        const int L = s.level[n];
+        if (threadIdx.x < 8) s_nb[threadIdx.x + 1] = s.nbr[8 * n + threadIdx.x];
+        __syncthreads();
+        const bool do_fill = (L >= lmin && L <= lmax);
+        if (do_fill) {
+            wait_done(s, q, (L > 0) ? s.lvl_off[L] : 0);
+            fill_hg_block(s, n, L, s_nb);
+        }
+        publish_done(s, q);
+        __syncthreads();
+        const int dx = s.dx[n];
+        const double cfl = 1.0 / (double)dx;
+        const bool shift = cfl > (double)0.9f;
+        const double cA = cfl / 2.0 * (1.0 + cfl), cB = 1.0 - cfl * cfl, cC = cfl / 2.0 * (1.0 - cfl);
+        for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+            const int x = c % nx + 1, y = c / nx + 1;
+            double csum = 0.0;
+#pragma unroll
+            for (int f = 0; f < 2; ++f) {
+                const double* A = f ? s.Ag : s.Ah;
+                double* B = f ? s.Bg : s.Bh;
+#pragma unroll
+                for (int i = 1; i <= 9; ++i) {
+                    double v;
+                    if (i == 1) {
+                        v = A[a_idx(s, n, 1, x, y)];
+                    } else if (shift) {
+                        v = A[a_idx(s, n, i, x - d_ex[i], y - d_ey[i])];
+                    } else {
+                        v = cA * A[a_idx(s, n, i, x - d_ex[i], y - d_ey[i])] +
+                            cB * A[a_idx(s, n, i, x, y)] -
+                            cC * A[a_idx(s, n, i, x + d_ex[i], y + d_ey[i])];
+                    }
+                    B[b_idx(s, n, i, x, y)] = v;
+                    if (f == 0) csum = csum + v;
+                }
+            }
+            s.C[c_idx(s, n, x, y)] = csum;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// grid-stride kernels over the leaf list (one CTA per block)
+
+__device__ __forceinline__ void load_tile(const DevState& s, int n, double* T) {
+    const int nx = s.nx, ny = s.ny, W = nx + 4, H = ny + 4;
+    for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x) {
+        const int x = idx % W - 2, y = idx / W - 2;
+        T[idx] = s.C[c_idx(s, n, x, y)];
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_collide(DevState s) {
+    extern __shared__ double T[];
+    const int nleaf = s.cnt->nleaf;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        atomicAdd(&s.cnt->updates, (unsigned long long)nleaf * (unsigned long long)(s.nx * s.ny));
+    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
+        const int n = s.leaf[m];
+        load_tile(s, n, T);
+        collide_consumer<CONS_COLLIDE_READ>(s, n, T);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_macro_g(DevState s) {
+    extern __shared__ double sm[];
+    double* T = sm;
+    double* red = sm + (s.nx + 4) * (s.ny + 4);
+    const int nleaf = s.cnt->nleaf;
+    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
+        const int n = s.leaf[m];
+        load_tile(s, n, T);
+        macro_g_err_consumer(s, n, T, red);
+        __syncthreads();
+    }
+}
+
+// Macroscopic_Values_h_AMR (LBM_Subroutines.f90:193-201)
+__global__ void k_macro_h(DevState s) {
+    const int nleaf = s.cnt->nleaf, nn = s.nx * s.ny;
+    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
+        const int n = s.leaf[m];
+        for (int c = threadIdx.x; c < nn; c += blockDim.x) {
+            const int x = c % s.nx + 1, y = c / s.nx + 1;
+            double sum = 0.0;
+#pragma unroll
+            for (int q = 1; q <= 9; ++q) sum = sum + s.Bh[b_idx(s, n, q, x, y)];
+            s.C[c_idx(s, n, x, y)] = sum;
+        }
+    }
+}
+
+// Err_Interface (Refine_Derefine.f90:327-351) of every leaf
+__global__ void k_err(DevState s) {
+    __shared__ double red[32];
+    const int nleaf = s.cnt->nleaf, nx = s.nx, ny = s.ny;
+    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
+        const int n = s.leaf[m];
+        double mx = 0.0;
+        for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+            const int x = c % nx + 1, y = c / nx + 1;
+            const double a = s.C[c_idx(s, n, x + 1, y)] - s.C[c_idx(s, n, x - 1, y)];
+            const double b = s.C[c_idx(s, n, x, y + 1)] - s.C[c_idx(s, n, x, y - 1)];
+            mx = fmax(mx, a * a + b * b);
+        }
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double r = 0.0;
+            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) r = fmax(r, red[w]);
+            s.err[n] = sqrt(r) / (2.0 * s.dx[n]);
+        }
+        __syncthreads();
+    }
+}
+
+// Initialize_AMR_Rising_Bubble (AMR_Rising_2D_OMP.f90:186-226) given C
+__global__ void __launch_bounds__(256) k_init_fields(DevState s, double R) {
+    extern __shared__ double T[];
+    const int nleaf = s.cnt->nleaf, nx = s.nx, ny = s.ny, TW = nx + 4;
+    const PhysD& ph = s.ph;
+    const double dRho3 = (ph.Rhoh - ph.Rhol) / 3.0;
+    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
+        const int n = s.leaf[m];
+        const int dx = s.dx[n];
+        load_tile(s, n, T);
+        for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+            const int x = c % nx + 1, y = c / nx + 1;
+            auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 2) * TW + (x + ddx + 2)]; };
+            const double Cij = Cs(0, 0);
+            const double Ux = 0, Uy = 0;
+            const double P = -ph.Sigma / R * Cij;
+            s.Ux[p_idx(s, n, x, y)] = Ux;
+            s.Uy[p_idx(s, n, x, y)] = Uy;
+            s.P[p_idx(s, n, x, y)] = P;
+            const double mu = chem_pot(ph, dx, Cs);
+            double E[10], Gamma[10], heq[10], DcDx, DcDy, ni, nj;
+            ed_c(dx, Cs, E);
+            gradient_ed(E, DcDx, DcDy);
+            normal_vec(DcDx, DcDy, ni, nj);
+            const double Rho = ph.Rhol + Cij * (ph.Rhoh - ph.Rhol);
+            const double Fb = 0;
+            equilibrium(ph, Cij, Ux, Uy, ni, nj, Gamma, heq);
+            const double ud = Ux * DcDx + Uy * DcDy;
+#pragma unroll
+            for (int k = 1; k <= 9; ++k) {
+                s.Bh[b_idx(s, n, k, x, y)] = heq[k];
+                const double hlp = ((Gamma[k] - wa(k)) * dRho3 + Gamma[k] * mu) * (E[k] - ud) +
+                                   ((double)d_ey[k] - Uy) * Gamma[k] * Fb;
+                s.Bg[b_idx(s, n, k, x, y)] = P * wa(k) + (Gamma[k] - wa(k)) * Rho / 3.0 - 0.5 * hlp;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// regrid (Refine_Derefine.f90): single-CTA topology passes + data kernels
+
+// value of a neighbour pointer with the dangling check
+__device__ __forceinline__ int resolve_chk(const DevState& s, int n, int k) {
+    const int o = s.nb_owner[8 * n + k - 1];
+    const int sl = s.nb_slot[8 * n + k - 1];
+    if (sl == 0) return o;
+    if (!s.child_alloc[o] || s.gen[o] != s.nb_gen[8 * n + k - 1]) set_error(s, 6, n);
+    return s.child[4 * o + sl - 1];
+}
+
+// Block-wide exclusive scan of a 0/1 flag; returns the prefix, *total gets the sum.
+__device__ int block_scan(int flag, int* total) {
+    __shared__ int warp_sums[32];
+    __shared__ int s_total;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned bal = __ballot_sync(0xffffffffu, flag);
+    const int pre = __popc(bal & ((1u << lane) - 1u));
+    if (lane == 0) warp_sums[wid] = __popc(bal);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int i = 0; i < nw; ++i) {
+            const int t = warp_sums[i];
+            warp_sums[i] = acc;
+            acc += t;
+        }
+        s_total = acc;
+    }
+    __syncthreads();
+    const int r = warp_sums[wid] + pre;
+    *total = s_total;
+    __syncthreads();
+    return r;
+}
+
+// Stable compaction over ids 1..nb of pred(id) into out[base..]; returns count.
+template <class Pred>
+__device__ int compact(int nb, int* out, int base, Pred pred) {
+    int count = 0;
+    for (int start = 1; start <= nb; start += blockDim.x) {
+        const int id = start + threadIdx.x;
+        const int f = (id <= nb) ? (pred(id) ? 1 : 0) : 0;
+        int tot;
+        const int pos = block_scan(f, &tot);
+        if (f) out[base + count + pos] = id;
+        count += tot;
+    }
+    return count;
+}
+
+// Check_Level_Jump_Deref_2D (Refine_Derefine.f90:169-194)
+__device__ __forceinline__ bool deref_ok(const DevState& s, int n, int dir, int c1, int c2) {
+    const int b = resolve_chk(s, n, dir);
+    if (b > 0 && !s.is_leaf[b]) {
+        int c = s.child[4 * b + c1 - 1];
+        for (int I = 1; I <= 2; ++I) {
+            if (s.refin[c] || (!s.is_leaf[c] && !s.deref[c])) return false;
+            c = s.child[4 * b + c2 - 1];
+        }
+    }
+    return true;
+}
+
+// Flag_for_refinement + Enforce_1_Level_Jump (:18-93), Flag_for_derefinement
+// + enforce_1_Level_jump_deref_2D (:97-165), and the list of blocks to
+// derefine in ascending id order (Derefine, :198-211).
+__global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_flags(DevState s, double refin_tol,
+                                                                    double deref_tol) {
+    const int nb = s.cnt->nblks;
+    const int lmin = s.cnt->level_min, lmax = s.cnt->level_max;
+    for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
+        uint8_t r = 0;
+        if (s.is_leaf[n]) {
+            if (s.level[n] < s.min_levels)
+                r = 1;
+            else if (s.level[n] < s.max_levels && s.err[n] > refin_tol)
+                r = 1;
+        }
+        s.refin[n] = r;
+    }
+    __syncthreads();
+    // closure: a refining block's coarser (Level-1) leaf neighbours refine too;
+    // processed from fine to coarse, every propagation goes one level down
+    for (int L = s.max_levels; L >= 1; --L) {
+        for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
+            if (s.level[n] != L || !s.refin[n]) continue;
+            for (int I = 1; I <= 8; ++I) {
+                const int b = resolve_chk(s, n, I);
+                if (b > 0 && s.level[b] == L - 1 && s.is_leaf[b]) s.refin[b] = 1;
+            }
+        }
+        __syncthreads();
+    }
+    for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
+        uint8_t d = 0;
+        if (s.has_leaf[n] && s.level[n] >= s.min_levels) {
+            const int c1 = s.child[4 * n];
+            if (!(s.refin[c1] || s.refin[c1 + 1] || s.refin[c1 + 2] || s.refin[c1 + 3])) {
+                d = 1;
+                for (int c = c1; c <= c1 + 3; ++c)
+                    if (s.err[c] > deref_tol) {
+                        d = 0;
+                        break;
+                    }
+            }
+        }
+        s.deref[n] = d;
+    }
+    __syncthreads();
+    for (int L = lmax - 1; L >= lmin - 1; --L) {
+        for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
+            if (s.level[n] != L || !s.deref[n]) continue;
+            const bool ok = deref_ok(s, n, 1, 2, 4) && deref_ok(s, n, 2, 1, 3) &&
+                            deref_ok(s, n, 3, 3, 4) && deref_ok(s, n, 4, 1, 2) &&
+                            deref_ok(s, n, 5, 4, 4) && deref_ok(s, n, 6, 2, 2) &&
+                            deref_ok(s, n, 7, 3, 3) && deref_ok(s, n, 8, 1, 1);
+            if (!ok) s.deref[n] = 0;
+        }
+        __syncthreads();
+    }
+    const int nd = compact(nb, s.der_list, 0, [&](int id) { return s.deref[id] != 0; });
+    if (threadIdx.x == 0) s.cnt->n_der = nd;
+}
+
+// Restrict_Bilinear (Restrict.f90:14-65) for every block in der_list: the
+// parent gets the 2x2 means of its children; ghost rings are zeroed.
+__global__ void k_restrict(DevState s) {
+    const int nd = s.cnt->n_der, nx = s.nx, ny = s.ny;
+    for (int i = blockIdx.x; i < nd; i += gridDim.x) {
+        const int par = s.der_list[i];
+        const int c1 = s.child[4 * par];
+        // zero C (all), P/U are written below, A rings
+        for (int idx = threadIdx.x; idx < s.cplane; idx += blockDim.x)
+            s.C[(size_t)par * s.cplane + idx] = 0.0;
+        const int R = 2 * (nx + ny) + 4;
+        for (int idx = threadIdx.x; idx < R * 18; idx += blockDim.x) {
+            const int r = idx % R, qf = idx / R;
+            int x, y;
+            ring1_xy(r, nx, ny, x, y);
+            double* A = (qf < 9) ? s.Ah : s.Ag;
+            A[a_idx(s, par, qf % 9 + 1, x, y)] = 0.0;
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+            const int x = c % nx + 1, y = c / nx + 1;
+            // fine cell (X,Y) of the 2nx x 2ny assembly of the children
+            auto F = [&](const double* base, int kind, int X, int Y, int q) {
+                const int ch = c1 + (X > nx ? 1 : 0) + (Y > ny ? 2 : 0);
+                const int xx = X > nx ? X - nx : X, yy = Y > ny ? Y - ny : Y;
+                if (kind == 0) return base[b_idx(s, ch, q, xx, yy)];
+                if (kind == 1) return base[c_idx(s, ch, xx, yy)];
+                return base[p_idx(s, ch, xx, yy)];
+            };
+            auto bil = [&](const double* base, int kind, int q) {
+                const double t0 = 0.5 * (F(base, kind, 2 * x - 1, 2 * y - 1, q) +
+                                         F(base, kind, 2 * x - 1, 2 * y, q));
+                const double t1 =
+                    0.5 * (F(base, kind, 2 * x, 2 * y - 1, q) + F(base, kind, 2 * x, 2 * y, q));
+                return 0.5 * (t0 + t1);
+            };
+            for (int q = 1; q <= 9; ++q) {
+                s.Bh[b_idx(s, par, q, x, y)] = bil(s.Bh, 0, q);
+                s.Bg[b_idx(s, par, q, x, y)] = bil(s.Bg, 0, q);
+            }
+            s.C[c_idx(s, par, x, y)] = bil(s.C, 1, 0);
+            s.P[p_idx(s, par, x, y)] = bil(s.P, 2, 0);
+            s.Ux[p_idx(s, par, x, y)] = bil(s.Ux, 2, 0);
+            s.Uy[p_idx(s, par, x, y)] = bil(s.Uy, 2, 0);
+        }
+        __syncthreads();
+    }
+}
+
+// Neighbor (Neighbors.f90:19-31)
+__device__ void set_ptr(const DevState& s, int n, int k, int owner, int slot) {
+    s.nb_owner[8 * n + k - 1] = owner;
+    s.nb_slot[8 * n + k - 1] = slot;
+    s.nb_gen[8 * n + k - 1] = slot ? s.gen[owner] : 0;
+}
+__device__ void copy_ptr(const DevState& s, int n, int k, int p) {
+    s.nb_owner[8 * n + k - 1] = s.nb_owner[8 * p + k - 1];
+    s.nb_slot[8 * n + k - 1] = s.nb_slot[8 * p + k - 1];
+    s.nb_gen[8 * n + k - 1] = s.nb_gen[8 * p + k - 1];
+}
+__device__ void neighbor(const DevState& s, int p, int n, int n2, int c) {
+    const int v = resolve_chk(s, p, n2);
+    if (v < 0)
+        copy_ptr(s, n, n2, p);
+    else
+        set_ptr(s, n, n2, v, c);
+    const int n1 = n2 + 1 - 2 * ((n2 - 1) % 2);
+    set_ptr(s, n, n1, p, c);
+}
+// through(k, slot): parent's pointer if negative, else child(slot) of it
+__device__ void diag_through(const DevState& s, int p, int n, int k, int slot) {
+    const int v = resolve_chk(s, p, k);
+    if (v < 0)
+        copy_ptr(s, n, k, p);
+    else
+        set_ptr(s, n, k, v, slot);
+}
+// fixed(kk, side, code, slot): the saved wall code if the side neighbour is external
+__device__ void diag_fixed(const DevState& s, int p, int n, int kk, int side, int code, int slot) {
+    const int v = resolve_chk(s, p, side);
+    if (v < 0)
+        set_ptr(s, n, kk, code, 0);
+    else
+        set_ptr(s, n, kk, v, slot);
+}
+// Find_Neighbors + Diagonal_Neighbor (Neighbors.f90:2-122)
+__device__ void find_neighbors(const DevState& s, int par, int n, int I, int J) {
+    const int c = 1 + I + 2 * J;
+    neighbor(s, par, n, 1 + I, c + 1 - 2 * I);
+    neighbor(s, par, n, 3 + J, c + 2 - 4 * J);
+    if (c == 1) {
+        diag_through(s, par, n, 5, 4);
+        diag_fixed(s, par, n, 6, 1, -6, 4);
+        diag_fixed(s, par, n, 7, 3, -7, 4);
+        set_ptr(s, n, 8, par, 4);
+    } else if (c == 2) {
+        diag_fixed(s, par, n, 5, 3, -5, 3);
+        set_ptr(s, n, 6, par, 3);
+        diag_through(s, par, n, 7, 3);
+        diag_fixed(s, par, n, 8, 2, -8, 3);
+    } else if (c == 3) {
+        diag_fixed(s, par, n, 5, 1, -5, 2);
+        diag_through(s, par, n, 6, 2);
+        set_ptr(s, n, 7, par, 2);
+        diag_fixed(s, par, n, 8, 4, -8, 2);
+    } else {
+        set_ptr(s, n, 5, par, 1);
+        diag_fixed(s, par, n, 6, 4, -6, 1);
+        diag_fixed(s, par, n, 7, 2, -7, 1);
+        diag_through(s, par, n, 8, 1);
+    }
+}
+
+// Remove_Children (:215-258), Refine (:262-294) with Add_Child_Blocks
+// (AMR_Rising_2D_OMP.f90:517-584), Array_of_Leaf_Blocks (:588-610) and the
+// neighbour table of the new leaves.
+__global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_topo(DevState s, int mode, int lmin_o,
+                                                                   int lmax_o, int set_levels) {
+    __shared__ int s_nr;
+    Counters* cnt = s.cnt;
+    const int nblks0 = cnt->nblks;
+    const int lmin = lmin_o >= 0 ? lmin_o : cnt->level_min;
+    const int lmax = lmax_o >= 0 ? lmax_o : cnt->level_max;
+    if (mode != 2) {
+        // ---- Derefine: Remove_Children for every listed parent (ascending ids)
+        const int nd = (mode == 0) ? cnt->n_der : 0;
+        const int head = cnt->fl_head, count = cnt->fl_count;
+        for (int i = threadIdx.x; i < nd; i += blockDim.x) {
+            const int par = s.der_list[i];
+            const int c1 = s.child[4 * par];
+            for (int c = c1; c <= c1 + 3; ++c) {
+                s.level[c] = -1;
+                s.is_leaf[c] = 0;
+                s.alloc[c] = 0;
+                s.child_alloc[c] = 0;
+                s.gen[c] = s.gen[c] + 1;
+            }
+            for (int k = 0; k < 4; ++k) s.child[4 * par + k] = par;
+            s.is_leaf[par] = 1;
+            s.has_leaf[par] = 0;
+            s.alloc[par] = 1;
+            s.freelist[(head + count + i) % s.fl_cap] = c1;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nd; i += blockDim.x) {
+            const int gp = s.parent[s.der_list[i]];
+            if (gp > 0) {
+                const int s1 = s.child[4 * gp], s4 = s.child[4 * gp + 3];
+                bool all = true;
+                for (int k = s1; k <= s4; ++k) all = all && s.is_leaf[k];
+                if (all) s.has_leaf[gp] = 1;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            cnt->fl_count = count + nd;
+            cnt->kk = cnt->kk + 4 * nd;
+        }
+        __syncthreads();
+        // ---- Refine: blocks in (level ascending, id ascending) order
+        int nr = 0;
+        for (int L = lmin; L <= lmax; ++L)
+            nr += compact(nblks0, s.ref_list, nr,
+                          [&](int id) { return s.level[id] == L && s.refin[id] != 0; });
+        const int F = cnt->fl_count, fh = cnt->fl_head;
+        if (threadIdx.x == 0) {
+            s_nr = nr;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < nr; k += blockDim.x) {
+            const int c1 = (k < F) ? s.freelist[(fh + k) % s.fl_cap] : nblks0 + 1 + 4 * (k - F);
+            if (c1 + 3 > s.max_blks) atomicMin(&s_nr, k);  // Add_Child_Blocks STOP
+            s.ref_c1[k] = c1;
+        }
+        __syncthreads();
+        if (s_nr < nr) {
+            if (threadIdx.x == 0) set_error(s, 3 /*AMRLBM_ERR_POOL_FULL*/, s_nr);
+            nr = s_nr;
+        }
+        const int used = nr < F ? nr : F;
+        if (threadIdx.x == 0) {
+            cnt->fl_head = (fh + used) % s.fl_cap;
+            cnt->fl_count = F - used;
+            cnt->kk = cnt->kk - 4 * used;
+            cnt->nblks = nr > F ? nblks0 + 4 * (nr - F) : nblks0;
+            cnt->n_ref = nr;
+            cnt->n_alloc_new = nr > F ? nr - F : 0;
+        }
+        for (int L = lmin; L <= lmax; ++L) {
+            for (int k = threadIdx.x; k < nr; k += blockDim.x) {
+                const int par = s.ref_list[k];
+                if (s.level[par] != L) continue;
+                const int c1 = s.ref_c1[k];
+                for (int i = 0; i < 4; ++i) s.child[4 * par + i] = c1 + i;
+                s.is_leaf[par] = 0;
+                s.has_leaf[par] = 1;
+                const int gp = s.parent[par];
+                if (gp > 0) s.has_leaf[gp] = 0;
+                if (mode == 0) s.alloc[par] = 0;  // Prolong_Bilinear deallocates
+                for (int J = 0; J <= 1; ++J)
+                    for (int I = 0; I <= 1; ++I) {
+                        const int N = c1 + I + 2 * J;
+                        s.level[N] = L + 1;
+                        s.dx[N] = s.dx[par] / 2;
+                        s.bi[N] = 2 * s.bi[par] + I;
+                        s.bj[N] = 2 * s.bj[par] + J;
+                        s.parent[N] = par;
+                        for (int q = 0; q < 4; ++q) s.child[4 * N + q] = N;
+                        s.child_alloc[N] = 1;
+                        find_neighbors(s, par, N, I, J);
+                        s.is_leaf[N] = 1;
+                        s.has_leaf[N] = 0;
+                        s.refin[N] = 0;
+                        s.deref[N] = 0;
+                        s.alloc[N] = 1;
+                    }
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    // ---- Array_of_Leaf_Blocks + per-level lists + resolved neighbours
+    const int nb = cnt->nblks;
+    const int nleaf = compact(nb, s.leaf, 0, [&](int id) { return s.is_leaf[id] != 0; });
+    int off = 0;
+    int lo = 1 << 30, hi = -(1 << 30);
+    for (int L = 0; L < AMR_MAXLV; ++L) {
+        if (threadIdx.x == 0) s.lvl_off[L] = off;
+        const int c = compact(nb, s.lvl_leaf, off,
+                              [&](int id) { return s.is_leaf[id] != 0 && s.level[id] == L; });
+        if (c > 0) {
+            lo = min(lo, L);
+            hi = max(hi, L);
+        }
+        off += c;
+    }
+    if (threadIdx.x == 0) {
+        s.lvl_off[AMR_MAXLV] = off;
+        cnt->nleaf = nleaf;
+        cnt->leaf_min = lo;
+        cnt->leaf_max = hi;
+        if (set_levels) {
+            cnt->level_min = lo;
+            cnt->level_max = hi;
+        }
+    }
+    for (int m = threadIdx.x; m < nleaf; m += blockDim.x) {
+        const int n = s.leaf[m];
+        for (int k = 1; k <= 8; ++k) s.nbr[8 * n + k - 1] = resolve_chk(s, n, k);
+    }
+}
+
+// Prolong_Bilinear (Prolong.f90:12-39) + Fill_Children_Data (:105-130) for
+// every refined block: children get bilinear h, g (with edge extrapolation)
+// and C (ring 1 included), zero ghost rings, then Macroscopic_Values_g_AMR.
+__global__ void __launch_bounds__(256) k_prolong(DevState s) {
+    extern __shared__ double T[];
+    const int nr = s.cnt->n_ref, nx = s.nx, ny = s.ny, TW = nx + 4;
+    for (int i = blockIdx.x; i < nr; i += gridDim.x) {
+        const int par = s.ref_list[i];
+        const int c1 = s.ref_c1[i];
+        for (int k = 0; k < 4; ++k) {
+            const int ch = c1 + k;
+            const int Ii = (k % 2) * nx, Jj = (k / 2) * ny;
+            // h, g: Bilinear_Interpolate_Extrapolate (Prolong.f90:43-70)
+            for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+                const int x = c % nx + 1, y = c / nx + 1;
+                const int xF = x + Ii, yF = y + Jj;
+                const int Xx = max(1, min(nx - 1, xF / 2)), ax = 2 * xF - 4 * Xx + 1, bx = 4 - ax;
+                const int Xy = max(1, min(ny - 1, yF / 2)), ay = 2 * yF - 4 * Xy + 1, by = 4 - ay;
+                for (int f = 0; f < 2; ++f) {
+                    const double* B = f ? s.Bg : s.Bh;
+                    double* Bo = f ? s.Bg : s.Bh;
+                    for (int q = 1; q <= 9; ++q) {
+                        const double t0 = (double)bx * B[b_idx(s, par, q, Xx, Xy)] +
+                                          (double)ax * B[b_idx(s, par, q, Xx + 1, Xy)];
+                        const double t1 = (double)bx * B[b_idx(s, par, q, Xx, Xy + 1)] +
+                                          (double)ax * B[b_idx(s, par, q, Xx + 1, Xy + 1)];
+                        Bo[b_idx(s, ch, q, x, y)] = ((double)by * t0 + (double)ay * t1) / 16.0;
+                    }
+                }
+            }
+            // C: Bilinear_Interpolation (Prolong.f90:74-101) on 0..nx+1, zero ring 2
+            const int W = nx + 4, H = ny + 4;
+            for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x) {
+                const int x = idx % W - 2, y = idx / W - 2;
+                double v = 0.0;
+                if (x >= 0 && x <= nx + 1 && y >= 0 && y <= ny + 1) {
+                    const int xF = x + Ii, yF = y + Jj;
+                    const int Xx = xF / 2, ax = 2 * xF - 4 * Xx + 1, bx = 4 - ax;
+                    const int Xy = yF / 2, ay = 2 * yF - 4 * Xy + 1, by = 4 - ay;
+                    const double t0 = (double)bx * s.C[c_idx(s, par, Xx, Xy)] +
+                                      (double)ax * s.C[c_idx(s, par, Xx + 1, Xy)];
+                    const double t1 = (double)bx * s.C[c_idx(s, par, Xx, Xy + 1)] +
+                                      (double)ax * s.C[c_idx(s, par, Xx + 1, Xy + 1)];
+                    v = ((double)by * t0 + (double)ay * t1) / 16.0;
+                }
+                s.C[c_idx(s, ch, x, y)] = v;
+                T[idx] = v;
+            }
+            const int R = 2 * (nx + ny) + 4;
+            for (int idx = threadIdx.x; idx < R * 18; idx += blockDim.x) {
+                const int r = idx % R, qf = idx / R;
+                int x, y;
+                ring1_xy(r, nx, ny, x, y);
+                double* A = (qf < 9) ? s.Ah : s.Ag;
+                A[a_idx(s, ch, qf % 9 + 1, x, y)] = 0.0;
+            }
+            __syncthreads();
+            // Macroscopic_Values_g_AMR of the child
+            const int dx = s.dx[ch];
+            for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+                const int x = c % nx + 1, y = c / nx + 1;
+                auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 2) * TW + (x + ddx + 2)]; };
+                double g[10];
+                for (int q = 1; q <= 9; ++q) g[q] = s.Bg[b_idx(s, ch, q, x, y)];
+                double P, Ux, Uy;
+                macro_g_cell(s.ph, dx, Cs, g, P, Ux, Uy);
+                s.P[p_idx(s, ch, x, y)] = P;
+                s.Ux[p_idx(s, ch, x, y)] = Ux;
+                s.Uy[p_idx(s, ch, x, y)] = Uy;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// zeroed fields of the children created by Initial_Mesh (Add_Child_Blocks,
+// AMR_Rising_2D_OMP.f90:572-577)
+__global__ void k_zero_children(DevState s) {
+    const int nr = s.cnt->n_ref;
+    for (int i = blockIdx.x; i < nr; i += gridDim.x) {
+        const int c1 = s.ref_c1[i];
+        for (int k = 0; k < 4; ++k) {
+            const int ch = c1 + k;
+            for (size_t idx = threadIdx.x; idx < (size_t)9 * s.bplane; idx += blockDim.x) {
+                s.Bh[(size_t)ch * 9 * s.bplane + idx] = 0.0;
+                s.Bg[(size_t)ch * 9 * s.bplane + idx] = 0.0;
+            }
+            for (size_t idx = threadIdx.x; idx < (size_t)9 * s.aplane; idx += blockDim.x) {
+                s.Ah[(size_t)ch * 9 * s.aplane + idx] = 0.0;
+                s.Ag[(size_t)ch * 9 * s.aplane + idx] = 0.0;
+            }
+            for (int idx = threadIdx.x; idx < s.cplane; idx += blockDim.x)
+                s.C[(size_t)ch * s.cplane + idx] = 0.0;
+            for (int idx = threadIdx.x; idx < s.pplane; idx += blockDim.x) {
+                s.P[(size_t)ch * s.pplane + idx] = 0.0;
+                s.Ux[(size_t)ch * s.pplane + idx] = 0.0;
+                s.Uy[(size_t)ch * s.pplane + idx] = 0.0;
+            }
+        }
+    }
+}
+
+// Initial_Mesh: every leaf of `level` refines
+__global__ void k_flag_level(DevState s, int level) {
+    const int nb = s.cnt->nblks;
+    for (int n = 1 + blockIdx.x * blockDim.x + threadIdx.x; n <= nb; n += gridDim.x * blockDim.x)
+        s.refin[n] = (s.level[n] == level && s.is_leaf[n]) ? 1 : 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.cnt->n_der = 0;
+}
+
+// Determine_Min_Max_Levels (AMR_Rising_2D_OMP.f90:434-452)
+__global__ void k_minmax(DevState s) {
+    __shared__ int lo, hi;
+    if (threadIdx.x == 0) {
+        lo = 100;
+        hi = -100;
+    }
+    __syncthreads();
+    const int nleaf = s.cnt->nleaf;
+    int l = 100, h = -100;
+    for (int m = threadIdx.x; m < nleaf; m += blockDim.x) {
+        const int L = s.level[s.leaf[m]];
+        l = min(l, L);
+        h = max(h, L);
+    }
+    atomicMin(&lo, l);
+    atomicMax(&hi, h);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s.cnt->level_min = lo;
+        s.cnt->level_max = hi;
+    }
+}
+
+// Output (AMR_Rising_2D_OMP.f90:456-489) with a fixed summation order: per
+// leaf block in (j,i) order, then over blocks in leaf-list order. out[8] =
+// non-finite flag. part: 8 doubles per leaf (scratch, >= 8*nleaf).
+__global__ void k_diag_blocks(DevState s, double* part) {
+    const int nleaf = s.cnt->nleaf, nx = s.nx, ny = s.ny;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < nleaf; m += gridDim.x * blockDim.x) {
+        const int n = s.leaf[m];
+        const int dx = s.dx[n];
+        const double a = (double)(dx * dx);
+        const PhysD& ph = s.ph;
+        double mass = 0, rmin = 10, rmax = -10, umax = 0, vol = 0, ysum = 0, vsum = 0, phase = 0;
+        bool finite = true;
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                const double C = s.C[c_idx(s, n, i, j)];
+                const double Rho = ph.Rhol + C * (ph.Rhoh - ph.Rhol);
+                rmin = fmin(rmin, Rho);
+                rmax = fmax(rmax, Rho);
+                mass = mass + Rho * a;
+                const double uy = s.Uy[p_idx(s, n, i, j)];
+                umax = fmax(umax, fabs(uy));
+                const double yc = (double)(s.bj[n] * dx * ny) + dx * (j - 0.5);
+                const double wgt = (1.0 - C) * a;
+                vol = vol + wgt;
+                ysum = ysum + wgt * yc;
+                vsum = vsum + wgt * uy;
+                phase = phase + C * a;
+                if (!isfinite(C) || !isfinite(uy)) finite = false;
+            }
+        double* o = part + 9 * (size_t)m;
+        o[0] = mass;
+        o[1] = rmin;
+        o[2] = rmax;
+        o[3] = umax;
+        o[4] = vol;
+        o[5] = ysum;
+        o[6] = vsum;
+        o[7] = phase;
+        o[8] = finite ? 0.0 : 1.0;
+    }
+}
+
+__global__ void k_diag_final(DevState s, const double* part, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int nleaf = s.cnt->nleaf;
+    double mass = 0, rmin = 10, rmax = -10, umax = 0, vol = 0, ysum = 0, vsum = 0, phase = 0, bad = 0;
+    for (int m = 0; m < nleaf; ++m) {
+        const double* o = part + 9 * (size_t)m;
+        mass = mass + o[0];
+        rmin = fmin(rmin, o[1]);
+        rmax = fmax(rmax, o[2]);
+        umax = fmax(umax, o[3]);
+        vol = vol + o[4];
+        ysum = ysum + o[5];
+        vsum = vsum + o[6];
+        phase = phase + o[7];
+        bad = bad + o[8];
+    }
+    out[0] = mass;
+    out[1] = rmin;
+    out[2] = rmax;
+    out[3] = umax;
+    out[4] = vol;
+    out[5] = ysum / vol;
+    out[6] = vsum / vol;
+    out[7] = phase;
+    out[8] = bad;
+}
+
+size_t tile_bytes(const DevState& s) { return (size_t)(s.nx + 4) * (s.ny + 4) * sizeof(double); }
+int block_threads(const DevState& s) {
+    const int t = ((s.nx * s.ny + 31) / 32) * 32;  // whole warps (shuffle reductions)
+    return t > 256 ? 256 : t;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+long long launches_issued() { return g_launches; }
+
+void launch_reset_queues(const DevState& s, cudaStream_t st) {
+    cudaMemsetAsync(s.queue, 0, sizeof(unsigned) * 2 * NQUEUES, st);
+}
+
+void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width,
+                   int consumer) {
+    const int q = (width == 2) ? Q_FILLC : Q_FILLC1;
+    cudaMemsetAsync(s.queue + 2 * q, 0, 2 * sizeof(unsigned), st);
+    const size_t sm = tile_bytes(s) + 32 * sizeof(double);
+    const int nt = block_threads(s);
+    switch (consumer) {
+        case CONS_NONE: k_fill_c<CONS_NONE><<<lc.grid_queue, nt, sm, st>>>(s, width, q); break;
+        case CONS_COLLIDE_READ:
+            k_fill_c<CONS_COLLIDE_READ><<<lc.grid_queue, nt, sm, st>>>(s, width, q);
+            break;
+        case CONS_COLLIDE_FUSED:
+            k_fill_c<CONS_COLLIDE_FUSED><<<lc.grid_queue, nt, sm, st>>>(s, width, q);
+            break;
+        default: k_fill_c<CONS_MACRO_G><<<lc.grid_queue, nt, sm, st>>>(s, width, q); break;
+    }
+    ++g_launches;
+}
+
+void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+    cudaMemsetAsync(s.queue + 2 * Q_FILLHG, 0, 2 * sizeof(unsigned), st);
+    k_fill_hg_stream<<<lc.grid_queue, block_threads(s), 0, st>>>(s);
+    ++g_launches;
+}
+
+void launch_collide(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+    k_collide<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s);
+    ++g_launches;
+}
+
+void launch_macro_h(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+    k_macro_h<<<lc.grid_leaves, block_threads(s), 0, st>>>(s);
+    ++g_launches;
+}
+
+void launch_macro_g(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+    k_macro_g<<<lc.grid_leaves, block_threads(s), tile_bytes(s) + 32 * sizeof(double), st>>>(s);
+    ++g_launches;
+}
+
+void launch_err(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+    k_err<<<lc.grid_leaves, block_threads(s), 0, st>>>(s);
+    ++g_launches;
+}
+
+void launch_minmax(const DevState& s, cudaStream_t st) {
+    k_minmax<<<1, 256, 0, st>>>(s);
+    ++g_launches;
+}
+
+void launch_init_fields(const DevState& s, const LaunchCfg& lc, cudaStream_t st, double radius) {
+    k_init_fields<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s, radius);
+    ++g_launches;
+}
+
+void launch_regrid_flags(const DevState& s, cudaStream_t st, double refin_tol, double deref_tol) {
+    k_regrid_flags<<<1, AMR_NTHREADS_TOPO, 0, st>>>(s, refin_tol, deref_tol);
+    ++g_launches;
+}
+
+void launch_restrict(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+    k_restrict<<<lc.grid_leaves, block_threads(s), 0, st>>>(s);
+    ++g_launches;
+}
+
+void launch_regrid_topo(const DevState& s, cudaStream_t st, int mode, int lmin, int lmax,
+                        int set_levels) {
+    k_regrid_topo<<<1, AMR_NTHREADS_TOPO, 0, st>>>(s, mode, lmin, lmax, set_levels);
+    ++g_launches;
+}
+
+void launch_prolong(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+    k_prolong<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s);
+    ++g_launches;
+}
+
+void launch_zero_children(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+    k_zero_children<<<lc.grid_leaves, 256, 0, st>>>(s);
+    ++g_launches;
+}
+
+void launch_flag_level(const DevState& s, cudaStream_t st, int level) {
+    k_flag_level<<<64, 256, 0, st>>>(s, level);
+    ++g_launches;
+}
+
+void launch_diag(const DevState& s, cudaStream_t st, double* out9) {
+    // out9: device buffer of 9 + 9*max_blks doubles
+    double* part = out9 + 9;
+    k_diag_blocks<<<64, 128, 0, st>>>(s, part);
+    k_diag_final<<<1, 32, 0, st>>>(s, part, out9);
+    g_launches += 2;
+}

@@ -1,0 +1,45 @@
+// amrlbm_launch.h - host-side launchers of the FP64 kernels (amrlbm_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "amrlbm_dev.cuh"
+
+// consumer work fused after a C ghost fill in one level-ordered launch
+enum FillCConsumer {
+    CONS_NONE = 0,          // Fill_Ghost_Cells_C / _C2 alone
+    CONS_COLLIDE_READ = 1,  // + Collision_h_g_AMR with P,Ux,Uy from memory
+    CONS_COLLIDE_FUSED = 2, // + Macroscopic_Values_g_AMR in registers + collision
+    CONS_MACRO_G = 3        // + Macroscopic_Values_g_AMR + Err_Interface
+};
+
+struct LaunchCfg {
+    int num_sms;
+    int grid_queue;     // CTAs of a level-ordered kernel
+    int grid_leaves;    // CTAs of a grid-stride kernel over leaves
+};
+
+void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width,
+                   int consumer);
+void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+void launch_collide(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+void launch_macro_h(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+void launch_macro_g(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+void launch_err(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+void launch_minmax(const DevState& s, cudaStream_t st);
+void launch_init_fields(const DevState& s, const LaunchCfg& lc, cudaStream_t st, double radius);
+void launch_regrid_flags(const DevState& s, cudaStream_t st, double refin_tol, double deref_tol);
+void launch_restrict(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+// mode 0: Refine_Derefine_Mesh; 1: Initial_Mesh level (no data movement);
+// 2: rebuild lists only. lmin/lmax < 0: take LevelMin/LevelMax from the
+// device counters. set_levels: LevelMin/LevelMax := level range of the new
+// leaves (what the next Determine_Min_Max_Levels returns).
+void launch_regrid_topo(const DevState& s, cudaStream_t st, int mode, int lmin, int lmax,
+                        int set_levels);
+void launch_prolong(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+void launch_zero_children(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+void launch_flag_level(const DevState& s, cudaStream_t st, int level);
+void launch_diag(const DevState& s, cudaStream_t st, double* out8);
+void launch_reset_queues(const DevState& s, cudaStream_t st);
+// number of kernels the launchers above issued (for the launch counter)
+long long launches_issued();

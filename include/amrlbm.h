@@ -1,0 +1,224 @@
+/*
+ * amrlbm.h - C ABI of the B200 (sm_100a) block-structured AMR two-phase
+ * lattice Boltzmann step (conservative phase field h + pressure/velocity g,
+ * D2Q9, weighted MRT) of the rising-bubble solver AMR-LBM-OpenMP-2D.
+ *
+ * The library owns ONE device-resident block pool. A caller (the reference's
+ * Fortran driver through ISO_C_BINDING, C, or Python through ctypes) keeps its
+ * own host arrays and copies them in and out only through the upload/download
+ * entry points below. Every entry point returns an int status: 0 = OK.
+ *
+ * Conventions shared with the reference (all cited paths are files of the
+ * reference project):
+ *   - block ids are 1-based Fortran indices into the pool Blk(1:MaxBlks)
+ *     (Parameters.f90:39);
+ *   - neighbour directions 1..8 = left, right, bottom, top, SW, NW, SE, NE
+ *     (AMR_Rising_2D_OMP.f90:97-101); a negative neighbour is an external
+ *     wall code;
+ *   - child slot k = 1 + I + 2J for the child at (I,J) in {0,1}^2
+ *     (AMR_Rising_2D_OMP.f90:542-551);
+ *   - populations 1..9 = rest, E, N, W, S, NE, NW, SW, SE (D2Q9_Mod.f90:6-7);
+ *   - field layouts are the reference's column-major arrays:
+ *       h, g : (9, 0:nx+1, 0:ny+1)          (Parameters.f90:36)
+ *       C    : (-1:nx+2, -1:ny+2)           (Parameters.f90:37)
+ *       P, Ux, Uy : (nx, ny)                (Parameters.f90:37)
+ *   - a neighbour is a POINTER to an integer, not a value
+ *     (Parameters.f90:23-31, Neighbors.f90:19-31). It is exported as the pair
+ *     (owner, slot): slot 1..4 means "child(slot) of block owner" and slot 0
+ *     means "the constant owner" (wall codes and the base blocks' own
+ *     neighbour integers). Its value is owner when slot == 0, else
+ *     child(slot) of owner at the time it is read.
+ *
+ * One context per host thread; calls on one context are not re-entrant. All
+ * device work of a context runs on that context's own CUDA stream.
+ */
+#ifndef AMRLBM_H
+#define AMRLBM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace the reference's PRINT / STOP) ---------------- */
+enum {
+    AMRLBM_OK = 0,
+    AMRLBM_ERR_ARG = 1,        /* bad argument or size                         */
+    AMRLBM_ERR_CUDA = 2,       /* CUDA runtime error / no device / no sm_100   */
+    AMRLBM_ERR_POOL_FULL = 3,  /* Add_Child_Blocks STOP, AMR_Rising_2D_OMP.f90:527-531 */
+    AMRLBM_ERR_LEVEL_JUMP = 4, /* "Error in SUB_Fill_*", Fill_Ghost_Cells_C.f90:85-87 */
+    AMRLBM_ERR_NAN = 5,        /* non-finite field value found by diagnostics  */
+    AMRLBM_ERR_DANGLING = 6,   /* neighbour pointer into a freed block's child array */
+    AMRLBM_ERR_STATE = 7,      /* call out of order (e.g. step before init)    */
+    AMRLBM_ERR_TIMEOUT = 8     /* a bounded device wait ran out                */
+};
+
+/* flag bits of amrlbm_get_topology / amrlbm_set_topology */
+enum {
+    AMRLBM_F_LEAF = 1,      /* Blk%IsLeaf  */
+    AMRLBM_F_HASLEAF = 2,   /* Blk%hasLeaf */
+    AMRLBM_F_REFIN = 4,     /* Blk%Refin   */
+    AMRLBM_F_DEREF = 8,     /* Blk%Deref   */
+    AMRLBM_F_ALLOC = 16     /* fields allocated (a leaf, or a derefined parent) */
+};
+
+/* Run-time parameters. The reference hard-codes these as PARAMETERs
+ * (Parameters.f90:12-19, D2Q9_Mod.f90:10-11) or literals
+ * (AMR_Rising_2D_OMP.f90:154-158,241-259,276-277); amrlbm_default_params()
+ * returns the reference's values. */
+typedef struct amrlbm_params {
+    int32_t nx, ny;          /* cells per block side (even, >= 4)                    */
+    int32_t nbx, nby;        /* base blocks in x (periodic) and y (walls)            */
+    int32_t dx0;             /* base-level cell size in finest cells (L0/nx)         */
+    int32_t min_levels;      /* minLevels                                            */
+    int32_t max_levels;      /* maxLevels                                            */
+    int32_t max_blks;        /* MaxBlks: pool capacity (blocks)                      */
+    int32_t regrid_every;    /* regrid after every n-th step (reference: 1)          */
+    int32_t reserved0;
+    double rho_l, rho_h;     /* Rhol, Rhoh                                            */
+    double visc_ratio;       /* muh/mul (reference: 100)                              */
+    double bo, ar;           /* Bond (=Eotvos) and Archimedes numbers                 */
+    double gy;               /* gravity                                               */
+    double w;                /* interface width W                                     */
+    double m0;               /* mobility M0                                           */
+    double radius, xc, yc;   /* bubble radius and centre (finest-cell units)          */
+    double refin_tol;        /* refine if Err_Interface > refin_tol                   */
+    double deref_tol;        /* derefine if all 4 children's error <= deref_tol       */
+} amrlbm_params;
+
+/* Derived physical constants (D2Q9_Mod.f90:13-16), as computed by
+ * Set_Rising_Bubble_Parameters (AMR_Rising_2D_OMP.f90:235-263). */
+typedef struct amrlbm_physics {
+    double w, sigma, beta, kappa, tau_l, tau_h, rho_l, rho_h, gy, m0;
+} amrlbm_physics;
+
+typedef struct amrlbm_ctx amrlbm_ctx;
+
+/* ---- set-up ------------------------------------------------------------- */
+void amrlbm_default_params(amrlbm_params* p);
+/* Set_Rising_Bubble_Parameters (AMR_Rising_2D_OMP.f90:235-263) for p. */
+int amrlbm_derive_physics(const amrlbm_params* p, amrlbm_physics* out);
+/* Allocates the device pool (max_blks blocks) on the current CUDA device. */
+int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out);
+int amrlbm_destroy(amrlbm_ctx* ctx);
+/* Replaces the derived constants (the Fortran driver computes its own). */
+int amrlbm_set_physics(amrlbm_ctx* ctx, const amrlbm_physics* phys);
+const char* amrlbm_last_error(const amrlbm_ctx* ctx);
+/* Device memory held by the context, bytes. */
+int64_t amrlbm_device_bytes(const amrlbm_ctx* ctx);
+
+/* ---- state transfer (host <-> device) ----------------------------------- */
+/* counts[0..4] = Nblks, nLeaf, KK, LevelMin, LevelMax (Parameters.f90:6-10) */
+int amrlbm_get_counts(amrlbm_ctx* ctx, int32_t counts[5]);
+/* Sets LevelMin/LevelMax as the driver does (AMR_Rising_2D_OMP.f90:51-52,66). */
+int amrlbm_set_level_range(amrlbm_ctx* ctx, int32_t level_min, int32_t level_max);
+/* Topology of blocks 1..nblks. Arrays are indexed by id-1; child has 4 entries
+ * per block, nbr_owner / nbr_slot 8 per block (pointer model above). The
+ * free list holds the first id of every freed quartet in FIFO order
+ * (Parameters.f90:41-45, Refine_Derefine.f90:246-254). */
+int amrlbm_set_topology(amrlbm_ctx* ctx, int32_t nblks, const int32_t* level,
+                        const int32_t* dx, const int32_t* bi, const int32_t* bj,
+                        const int32_t* parent, const int32_t* child,
+                        const int32_t* nbr_owner, const int32_t* nbr_slot,
+                        const uint8_t* flags, int32_t n_free, const int32_t* free_list,
+                        int32_t kk);
+int amrlbm_get_topology(amrlbm_ctx* ctx, int32_t* level, int32_t* dx, int32_t* bi,
+                        int32_t* bj, int32_t* parent, int32_t* child,
+                        int32_t* nbr_owner, int32_t* nbr_slot, uint8_t* flags,
+                        int32_t* n_free, int32_t* free_list);
+/* Resolved neighbour ids nbr[8*(id-1)+k-1] = Blk(id)%nghbr(k)%n of blocks
+ * 1..Nblks (0 for blocks without fields). */
+int amrlbm_get_neighbours(amrlbm_ctx* ctx, int32_t* nbr);
+/* Leaf list LeafBlks(1:nLeaf) (AMR_Rising_2D_OMP.f90:588-610). */
+int amrlbm_get_leaves(amrlbm_ctx* ctx, int32_t* leaves);
+/* One block's fields in the reference layouts; any pointer may be NULL. */
+int amrlbm_upload_block(amrlbm_ctx* ctx, int32_t id, const double* h, const double* g,
+                        const double* C, const double* P, const double* Ux,
+                        const double* Uy);
+int amrlbm_download_block(amrlbm_ctx* ctx, int32_t id, double* h, double* g, double* C,
+                          double* P, double* Ux, double* Uy);
+/* Bulk transfer of n blocks ids[0..n-1]: each array holds n consecutive
+ * blocks in the per-block layout above. Any field pointer may be NULL. */
+int amrlbm_upload_fields(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, const double* h,
+                         const double* g, const double* C, const double* P,
+                         const double* Ux, const double* Uy);
+int amrlbm_download_fields(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, double* h,
+                           double* g, double* C, double* P, double* Ux, double* Uy);
+/* Per-block interface error Err_Interface (Refine_Derefine.f90:327-351) of
+ * blocks 1..Nblks as last computed by amrlbm_macro_g / amrlbm_regrid
+ * (0 for blocks that are not leaves). */
+int amrlbm_get_block_error(amrlbm_ctx* ctx, double* err);
+
+/* ---- driver helpers ----------------------------------------------------- */
+/* The reference driver's start-up, AMR_LBM_Rising_Bubble
+ * (AMR_Rising_2D_OMP.f90:49-67): base blocks (generalised to nbx x nby,
+ * periodic in x, walls in y), Initial_Mesh, the analytic bubble of
+ * Initialize_AMR_Rising_Bubble and the start-up regrid loop. The tanh/sqrt
+ * profile is evaluated on the host (as the driver does); everything else runs
+ * on the device. */
+int amrlbm_init_rising_bubble(amrlbm_ctx* ctx);
+/* Initialize_AMR_Rising_Bubble (AMR_Rising_2D_OMP.f90:142-231) alone, for the
+ * current leaves. */
+int amrlbm_init_fields(amrlbm_ctx* ctx);
+
+/* ---- phase entry points (the Main_Loop call sites) ---------------------- */
+/* Determine_Min_Max_Levels (AMR_Rising_2D_OMP.f90:304,434-452). */
+int amrlbm_min_max_levels(amrlbm_ctx* ctx, int32_t* level_min, int32_t* level_max);
+/* Fill_Ghost_Cells_C2 (AMR_Rising_2D_OMP.f90:318). */
+int amrlbm_fill_ghost_c2(amrlbm_ctx* ctx);
+/* Phase_Field_LBM_h_g_AMR: collide all leaves, Fill_Ghost_Cells_hg, stream
+ * (AMR_Rising_2D_OMP.f90:322,381-430). */
+int amrlbm_phase_field_step(amrlbm_ctx* ctx);
+/* Macroscopic_Values_h_AMR over leaves (AMR_Rising_2D_OMP.f90:328-335). */
+int amrlbm_macro_h(amrlbm_ctx* ctx);
+/* Fill_Ghost_Cells_C (AMR_Rising_2D_OMP.f90:341). */
+int amrlbm_fill_ghost_c(amrlbm_ctx* ctx);
+/* Macroscopic_Values_g_AMR over leaves (AMR_Rising_2D_OMP.f90:346-354);
+ * also computes every leaf's Err_Interface for the next regrid. */
+int amrlbm_macro_g(amrlbm_ctx* ctx);
+/* Refine_Derefine_Mesh (AMR_Rising_2D_OMP.f90:360, Refine_Derefine.f90:2-14). */
+int amrlbm_regrid(amrlbm_ctx* ctx, double refin_tol, double deref_tol);
+/* nsteps iterations of the Main_Loop body (AMR_Rising_2D_OMP.f90:304-363)
+ * without output, regridding after every regrid_every-th step (counted over
+ * the context's lifetime). Steps that are not followed by a regrid run the
+ * fused path (the next step's Fill_Ghost_Cells_C2 supplies the ring that
+ * Fill_Ghost_Cells_C would write; Macroscopic_Values_g_AMR runs inside the
+ * collision); on return the state equals the reference's at a step boundary.
+ * Runs as CUDA graphs; does not synchronise the host. */
+int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps);
+/* Blocks the host until the context's stream is idle; returns a pending
+ * device error status (pool full, level jump, ...), if any. */
+int amrlbm_sync(amrlbm_ctx* ctx);
+
+/* ---- diagnostics -------------------------------------------------------- */
+/* Output (AMR_Rising_2D_OMP.f90:456-489) with a fixed summation order, plus
+ * the bubble (C < 1/2) centroid and rise velocity:
+ *   out[0] mass = sum rho*dx^2       out[1] rho_min   out[2] rho_max
+ *   out[3] u_max = max |Uy|          out[4] bubble volume = sum (1-C)*dx^2
+ *   out[5] yc = sum (1-C)*y*dx^2 / out[4]
+ *   out[6] v_rise = sum (1-C)*Uy*dx^2 / out[4]
+ *   out[7] phase volume sum C*dx^2
+ * Returns AMRLBM_ERR_NAN if any leaf value is not finite. */
+int amrlbm_diag(amrlbm_ctx* ctx, double out[8]);
+
+/* ---- timing (CUDA events on the context's stream) ----------------------- */
+int amrlbm_timer_start(amrlbm_ctx* ctx);
+/* Milliseconds since amrlbm_timer_start; synchronises. */
+int amrlbm_timer_stop(amrlbm_ctx* ctx, float* ms);
+/* Per-kernel device time accounting of amrlbm_step: when enabled, every
+ * launch of the collision kernel is bracketed by CUDA events on the
+ * launching stream. kernel_ms returns the accumulated time and launches. */
+int amrlbm_profile_enable(amrlbm_ctx* ctx, int32_t enable);
+int amrlbm_profile_read(amrlbm_ctx* ctx, int32_t kernel, double* total_ms,
+                        int64_t* launches, int64_t* cells);
+/* Number of kernels this library launched since creation. */
+int64_t amrlbm_launch_count(const amrlbm_ctx* ctx);
+/* Writes a buffer larger than the L2 cache on the context's stream. */
+int amrlbm_flush_l2(amrlbm_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AMRLBM_H */

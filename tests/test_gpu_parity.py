@@ -1,0 +1,196 @@
+"""Parity of the B200 path with the CPU oracle, through the C ABI.
+
+Every test runs the same inputs through libamrlbm.so (amrlbm.AmrLbm) and the
+oracle and requires identical integer state and identical FP64 fields
+(tolerance 0: the north-star bound is 1e-12 relative; the device path meets
+it exactly because it keeps the reference's operation order without FMA).
+"""
+import numpy as np
+import pytest
+
+import amrlbm
+from amrlbm import AmrLbm, AmrLbmError
+from oracle_lib import Oracle
+from parity import (compare_counts, compare_fields, compare_state, compare_topology,
+                    copy_state_to_gpu, randomize_leaves)
+
+pytestmark = pytest.mark.gpu
+
+
+def tiny_params(**kw):
+    """Small rising bubble with 8x8 blocks: 2x4 base blocks, 3 levels."""
+    p = amrlbm.bubble_params(16, 32, 3, radius=10.0, xc=64.0, yc=80.0, rho_ratio=1000.0,
+                             visc_ratio=100.0, eo=10.0, mo=1e-5, n=8, regrid_every=1)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+CASES = {
+    "reference_default": amrlbm.reference_params,
+    "tiny_minlevels0": tiny_params,
+    "small_16x16": amrlbm.workload_small,
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_init_parity(case):
+    p = CASES[case]()
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    with AmrLbm(p) as gpu:
+        gpu.initialize_rising_bubble()
+        compare_state(gpu, orc)
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_phase_by_phase(case):
+    """Main_Loop call sites one by one (AMR_Rising_2D_OMP.f90:304-360)."""
+    p = CASES[case]()
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    with AmrLbm(p) as gpu:
+        gpu.initialize_rising_bubble()
+        for step in range(3):
+            assert gpu.determine_min_max_levels() == orc.determine_min_max_levels()
+            orc.fill_ghost_cells_c2()
+            gpu.fill_ghost_cells_c2()
+            compare_fields(gpu, orc, fields=("C",))
+            orc.phase_field_lbm_h_g()
+            gpu.phase_field_lbm_h_g()
+            compare_fields(gpu, orc, fields=("h", "g"))
+            orc.macroscopic_values_h()
+            gpu.macroscopic_values_h()
+            compare_fields(gpu, orc, fields=("C",))
+            orc.fill_ghost_cells_c()
+            gpu.fill_ghost_cells_c()
+            compare_fields(gpu, orc, fields=("C",))
+            orc.macroscopic_values_g()
+            gpu.macroscopic_values_g()
+            compare_fields(gpu, orc, fields=("P", "Ux", "Uy"))
+            errs = gpu.block_errors()
+            for bid in orc.leaves():
+                assert errs[bid - 1] == orc.block_error(int(bid))
+            orc.refine_derefine_mesh()
+            gpu.refine_derefine_mesh()
+            compare_state(gpu, orc)
+
+
+@pytest.mark.parametrize("case,regrid_every,nsteps", [
+    ("reference_default", 1, 12),
+    ("tiny_minlevels0", 1, 15),
+    ("tiny_minlevels0", 4, 13),
+    ("small_16x16", 3, 10),
+])
+def test_main_loop_parity(case, regrid_every, nsteps):
+    """amrlbm_step (fused, graph-captured) against the oracle's Main_Loop body."""
+    p = CASES[case]()
+    p.regrid_every = regrid_every
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    with AmrLbm(p) as gpu:
+        gpu.initialize_rising_bubble()
+        orc.main_loop(nsteps)
+        gpu.main_loop(nsteps)
+        gpu.sync()
+        compare_state(gpu, orc)
+        # a second call continues the same trajectory
+        orc.main_loop(5)
+        gpu.main_loop(5)
+        gpu.sync()
+        compare_state(gpu, orc)
+
+
+def test_random_fields_all_branches():
+    """Random C outside [0,1] (both tau clamps), random P, U, h, g on a
+    3-level mesh; every phase and the regrid must agree."""
+    p = tiny_params()
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    randomize_leaves(orc, seed=20261203)
+    with AmrLbm(p) as gpu:
+        copy_state_to_gpu(orc, gpu)
+        compare_state(gpu, orc)
+        orc.fill_ghost_cells_c2()
+        gpu.fill_ghost_cells_c2()
+        compare_fields(gpu, orc, fields=("C",))
+        orc.phase_field_lbm_h_g()
+        gpu.phase_field_lbm_h_g()
+        compare_fields(gpu, orc, fields=("h", "g"))
+        for f in ("macroscopic_values_h", "fill_ghost_cells_c", "macroscopic_values_g"):
+            getattr(orc, f)()
+            getattr(gpu, f)()
+        compare_fields(gpu, orc)
+        orc.refine_derefine_mesh()
+        gpu.refine_derefine_mesh()
+        compare_state(gpu, orc)
+
+
+def test_diagnostics_match():
+    p = tiny_params()
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    with AmrLbm(p) as gpu:
+        gpu.initialize_rising_bubble()
+        orc.main_loop(7)
+        gpu.main_loop(7)
+        a, b = gpu.output(), orc.output()
+        for k in a:
+            assert a[k] == b[k], (k, a[k], b[k])
+
+
+def test_pool_full_is_reported():
+    """Add_Child_Blocks STOP (AMR_Rising_2D_OMP.f90:527-531) -> status code."""
+    p = tiny_params(max_blks=20)
+    orc = Oracle(p)
+    with pytest.raises(AssertionError):
+        orc.initialize_rising_bubble()
+    assert orc.error() == amrlbm.ERR_POOL_FULL
+    with AmrLbm(p) as gpu:
+        with pytest.raises(AmrLbmError) as ei:
+            gpu.initialize_rising_bubble()
+        assert ei.value.status == amrlbm.ERR_POOL_FULL
+
+
+def test_level_jump_is_reported():
+    """A leaf whose neighbour is two levels coarser: the reference prints
+    "Error in SUB_Fill_*" and leaves the ghost cells; the device reports
+    AMRLBM_ERR_LEVEL_JUMP and leaves them too."""
+    p = tiny_params()
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    t = orc.topology()
+    lv = t["level"]
+    leaves = orc.leaves()
+    deep = [b for b in leaves if lv[b - 1] == lv.max()]
+    coarse = [b for b in leaves if lv[b - 1] <= lv.max() - 2]
+    assert deep and coarse
+    b = deep[0]
+    t["nbr_owner"][b - 1, 0] = coarse[0]   # left neighbour pointer -> constant coarse id
+    t["nbr_slot"][b - 1, 0] = 0
+    orc.set_topology(t, orc.counts()["kk"])
+    with AmrLbm(p) as gpu:
+        copy_state_to_gpu(orc, gpu)
+        orc.fill_ghost_cells_c2()
+        assert orc.level_jumps() > 0
+        with pytest.raises(AmrLbmError) as ei:
+            gpu.fill_ghost_cells_c2()
+        assert ei.value.status == amrlbm.ERR_LEVEL_JUMP
+        compare_fields(gpu, orc, fields=("C",))
+
+
+def test_large_workload_topology_and_fields():
+    """The 256x512-base, 3-level, R=128 workload at full size: start-up and
+    20 steps with a regrid every 10."""
+    p = amrlbm.workload_large()
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    with AmrLbm(p) as gpu:
+        gpu.initialize_rising_bubble()
+        compare_state(gpu, orc)
+        orc.main_loop(20)
+        gpu.main_loop(20)
+        gpu.sync()
+        compare_counts(gpu, orc)
+        compare_topology(gpu, orc)
+        compare_fields(gpu, orc)
