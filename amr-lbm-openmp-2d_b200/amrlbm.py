@@ -403,11 +403,15 @@ class AmrLbm:
             self.ctx, bid, *[_ptr(a, ct.c_double) for a in arrs]))
 
     def download_fields(self, ids):
+        """Fields of blocks `ids` as flat per-block records (n, size) in the
+        reference's column-major layouts; reshape a record with order="F"."""
         ids = np.ascontiguousarray(ids, dtype=np.int32)
         n = len(ids)
-        out = dict(h=np.zeros((n,) + self.hshape[::-1]), g=np.zeros((n,) + self.hshape[::-1]),
-                   C=np.zeros((n,) + self.cshape[::-1]), P=np.zeros((n,) + self.pshape[::-1]),
-                   Ux=np.zeros((n,) + self.pshape[::-1]), Uy=np.zeros((n,) + self.pshape[::-1]))
+        hs = int(np.prod(self.hshape))
+        cs = int(np.prod(self.cshape))
+        ps = int(np.prod(self.pshape))
+        out = dict(h=np.zeros((n, hs)), g=np.zeros((n, hs)), C=np.zeros((n, cs)),
+                   P=np.zeros((n, ps)), Ux=np.zeros((n, ps)), Uy=np.zeros((n, ps)))
         self._check(self.lib.amrlbm_download_fields(
             self.ctx, n, _ptr(ids, ct.c_int32),
             *[_ptr(out[k], ct.c_double) for k in ("h", "g", "C", "P", "Ux", "Uy")]))

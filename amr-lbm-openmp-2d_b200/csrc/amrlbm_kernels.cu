@@ -141,7 +141,7 @@ __device__ __forceinline__ int ghost_dir(int x, int y, int nx, int ny) {
 }
 
 // Fills the C ring of width w of block n into global memory and into the
-// shared tile T ((nx+4) x (ny+4), index (y+2)*(nx+4)+(x+2)); the interior of
+// shared tile T ((nx+4) x (ny+4), index (y+1)*(nx+4)+(x+1)); the interior of
 // T must already be loaded. Ends with the ring complete in T and in memory.
 __device__ void fill_c_block(const DevState& s, int n, int L, const int* nb, int w,
                              double* T) {
@@ -160,7 +160,7 @@ __device__ void fill_c_block(const DevState& s, int n, int L, const int* nb, int
             continue;
         }
         s.C[c_idx(s, n, x, y)] = v;
-        T[(y + 2) * TW + (x + 2)] = v;
+        T[(y + 1) * TW + (x + 1)] = v;
     }
     __syncthreads();
     // Symmetric_C(2)_3/4 (BC_Cell.f90:46-104): overwrite the wall rows
@@ -168,8 +168,8 @@ __device__ void fill_c_block(const DevState& s, int n, int L, const int* nb, int
         for (int X = threadIdx.x - (w - 1); X <= nx + w; X += blockDim.x) {
             if (X < 1 - w) continue;
             for (int a = 1; a <= w; ++a) {  // C(X,1-a) = C(X,a)
-                const double v = T[(a + 2) * TW + (X + 2)];
-                T[(1 - a + 2) * TW + (X + 2)] = v;
+                const double v = T[(a + 1) * TW + (X + 1)];
+                T[(1 - a + 1) * TW + (X + 1)] = v;
                 s.C[c_idx(s, n, X, 1 - a)] = v;
             }
         }
@@ -178,8 +178,8 @@ __device__ void fill_c_block(const DevState& s, int n, int L, const int* nb, int
         for (int X = threadIdx.x - (w - 1); X <= nx + w; X += blockDim.x) {
             if (X < 1 - w) continue;
             for (int a = 1; a <= w; ++a) {  // C(X,ny+a) = C(X,ny+1-a)
-                const double v = T[(ny + 1 - a + 2) * TW + (X + 2)];
-                T[(ny + a + 2) * TW + (X + 2)] = v;
+                const double v = T[(ny + 1 - a + 1) * TW + (X + 1)];
+                T[(ny + a + 1) * TW + (X + 1)] = v;
                 s.C[c_idx(s, n, X, ny + a)] = v;
             }
         }
@@ -324,7 +324,7 @@ __device__ __forceinline__ void collide_consumer(const DevState& s, int n, const
     const int dx = s.dx[n];
     for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
         const int x = c % nx + 1, y = c / nx + 1;
-        auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 2) * TW + (x + ddx + 2)]; };
+        auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 1) * TW + (x + ddx + 1)]; };
         double h[10], g[10];
 #pragma unroll
         for (int q = 1; q <= 9; ++q) {
@@ -355,7 +355,7 @@ __device__ void macro_g_err_consumer(const DevState& s, int n, const double* T, 
     double mx = 0.0;
     for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
         const int x = c % nx + 1, y = c / nx + 1;
-        auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 2) * TW + (x + ddx + 2)]; };
+        auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 1) * TW + (x + ddx + 1)]; };
         double g[10];
 #pragma unroll
         for (int q = 1; q <= 9; ++q) g[q] = s.Bg[b_idx(s, n, q, x, y)];
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256) k_fill_c(DevState s, int w, int q) {
         {
             const int W = nx + 4, H = ny + 4;
             for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x)
-                T[idx] = ldcg(&s.C[c_idx(s, n, idx % W - 2, idx / W - 2)]);
+                T[idx] = ldcg(&s.C[c_idx(s, n, idx % W - 1, idx / W - 1)]);
         }
         const bool do_fill = (L >= lmin && L <= lmax);
         if (do_fill) {
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(256) k_fill_hg_stream(DevState s) {
 __device__ __forceinline__ void load_tile(const DevState& s, int n, double* T) {
     const int nx = s.nx, ny = s.ny, W = nx + 4, H = ny + 4;
     for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x) {
-        const int x = idx % W - 2, y = idx / W - 2;
+        const int x = idx % W - 1, y = idx / W - 1;
         T[idx] = s.C[c_idx(s, n, x, y)];
     }
     __syncthreads();
@@ -570,7 +570,7 @@ __global__ void __launch_bounds__(256) k_init_fields(DevState s, double R) {
         load_tile(s, n, T);
         for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
             const int x = c % nx + 1, y = c / nx + 1;
-            auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 2) * TW + (x + ddx + 2)]; };
+            auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 1) * TW + (x + ddx + 1)]; };
             const double Cij = Cs(0, 0);
             const double Ux = 0, Uy = 0;
             const double P = -ph.Sigma / R * Cij;
@@ -1010,7 +1010,7 @@ __global__ void __launch_bounds__(256) k_prolong(DevState s) {
             // C: Bilinear_Interpolation (Prolong.f90:74-101) on 0..nx+1, zero ring 2
             const int W = nx + 4, H = ny + 4;
             for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x) {
-                const int x = idx % W - 2, y = idx / W - 2;
+                const int x = idx % W - 1, y = idx / W - 1;
                 double v = 0.0;
                 if (x >= 0 && x <= nx + 1 && y >= 0 && y <= ny + 1) {
                     const int xF = x + Ii, yF = y + Jj;
@@ -1038,7 +1038,7 @@ __global__ void __launch_bounds__(256) k_prolong(DevState s) {
             const int dx = s.dx[ch];
             for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
                 const int x = c % nx + 1, y = c / nx + 1;
-                auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 2) * TW + (x + ddx + 2)]; };
+                auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 1) * TW + (x + ddx + 1)]; };
                 double g[10];
                 for (int q = 1; q <= 9; ++q) g[q] = s.Bg[b_idx(s, ch, q, x, y)];
                 double P, Ux, Uy;
