@@ -49,7 +49,7 @@ class Params(ct.Structure):
         ("dx0", ct.c_int32),
         ("min_levels", ct.c_int32), ("max_levels", ct.c_int32),
         ("max_blks", ct.c_int32),
-        ("regrid_every", ct.c_int32), ("reserved0", ct.c_int32),
+        ("regrid_every", ct.c_int32), ("device", ct.c_int32),
         ("rho_l", ct.c_double), ("rho_h", ct.c_double),
         ("visc_ratio", ct.c_double),
         ("bo", ct.c_double), ("ar", ct.c_double),
@@ -60,7 +60,7 @@ class Params(ct.Structure):
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved0"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Physics(ct.Structure):

@@ -20,6 +20,7 @@ size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
 
 struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;  // kernels captured in the graph
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof;  // (kernel, events)
 };
 
@@ -49,6 +50,10 @@ struct amrlbm_ctx {
     long long prof_cells[4] = {0, 0, 0, 0};
     std::map<std::tuple<int, int, int, int, int>, GraphEntry> graphs;
     long long launches0 = 0;
+    long long captured = 0, replayed = 0;  // graph kernels: captured once, run per replay
+    GraphEntry* prof_pending = nullptr;    // replayed with profiling, events not read yet
+    double* h_stage = nullptr;             // pinned host staging
+    size_t h_stage_doubles = 0;
 };
 
 namespace {
@@ -171,6 +176,12 @@ int ensure_stage(amrlbm_ctx* ctx, size_t nblocks) {
         CK(cudaMalloc(&ctx->d_stage, need * sizeof(double)));
         ctx->stage_doubles = need;
     }
+    if (need > ctx->h_stage_doubles) {
+        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+        ctx->h_stage = nullptr;
+        CK(cudaMallocHost(&ctx->h_stage, need * sizeof(double)));
+        ctx->h_stage_doubles = need;
+    }
     if (nblocks > ctx->ids_cap) {
         if (ctx->d_ids) cudaFree(ctx->d_ids);
         ctx->d_ids = nullptr;
@@ -194,9 +205,24 @@ int device_error(amrlbm_ctx* ctx) {
     return fail(ctx, e[0], std::string("device: ") + nm + " (info " + std::to_string(e[1]) + ")");
 }
 
+// reads the kernel events of the last profiled graph replay (stream idle)
+void harvest_profile(amrlbm_ctx* ctx) {
+    GraphEntry* ge = ctx->prof_pending;
+    ctx->prof_pending = nullptr;
+    if (!ge) return;
+    for (auto& pe : ge->prof) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess) {
+            ctx->prof_ms[pe.first] += ms;
+            ctx->prof_n[pe.first] += 1;
+        }
+    }
+}
+
 int sync_check(amrlbm_ctx* ctx) {
     CK(cudaStreamSynchronize(ctx->st));
     CK(cudaGetLastError());
+    harvest_profile(ctx);
     return device_error(ctx);
 }
 
@@ -352,6 +378,7 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
         return AMRLBM_ERR_ARG;
     if ((p->dx0 >> p->max_levels) < 1) return AMRLBM_ERR_ARG;  // dx stays an integer >= 1
     int dev = 0, cc = 0, sms = 0;
+    if (p->device >= 0 && cudaSetDevice(p->device) != cudaSuccess) return AMRLBM_ERR_CUDA;
     if (cudaGetDevice(&dev) != cudaSuccess) return AMRLBM_ERR_CUDA;
     cudaDeviceGetAttribute(&cc, cudaDevAttrComputeCapabilityMajor, dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -456,6 +483,7 @@ int amrlbm_destroy(amrlbm_ctx* ctx) {
     if (ctx->d_stage) cudaFree(ctx->d_stage);
     if (ctx->d_ids) cudaFree(ctx->d_ids);
     if (ctx->d_flush) cudaFree(ctx->d_flush);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     if (ctx->t0) cudaEventDestroy(ctx->t0);
     if (ctx->t1) cudaEventDestroy(ctx->t1);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -667,13 +695,13 @@ int amrlbm_download_fields(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, doubl
     k_transfer<<<ctx->lc.grid_leaves, 256, 0, ctx->st>>>(ctx->s, ctx->d_ids, n, ctx->d_stage, 1,
                                                          mask, L);
     CK(cudaGetLastError());
-    std::vector<double> host((size_t)n * L.per);
-    CK(cudaMemcpyAsync(host.data(), ctx->d_stage, host.size() * 8, cudaMemcpyDeviceToHost,
+    double* host = ctx->h_stage;
+    CK(cudaMemcpyAsync(host, ctx->d_stage, (size_t)n * L.per * 8, cudaMemcpyDeviceToHost,
                        ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     const size_t hs = L.g - L.h, cs = L.P - L.C, ps = L.Ux - L.P;
     for (int i = 0; i < n; ++i) {
-        const double* rec = host.data() + (size_t)i * L.per;
+        const double* rec = host + (size_t)i * L.per;
         if (h) std::memcpy(h + i * hs, rec + L.h, hs * 8);
         if (g) std::memcpy(g + i * hs, rec + L.g, hs * 8);
         if (C) std::memcpy(C + i * cs, rec + L.C, cs * 8);
@@ -869,9 +897,14 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
         const bool final_chunk = (done + chunk == nsteps);
         const auto key = std::make_tuple(chunk, phase, ctx->tail_done ? 1 : 0, final_chunk ? 1 : 0,
                                          ctx->prof ? 1 : 0);
+        if (ctx->prof_pending) {  // the previous replay's events must be read first
+            CK(cudaStreamSynchronize(ctx->st));
+            harvest_profile(ctx);
+        }
         auto it = ctx->graphs.find(key);
         if (it == ctx->graphs.end()) {
             GraphEntry ge;
+            const long long k0 = launches_issued();
             CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
             bool prev_tail = ctx->tail_done;
             for (int t = 0; t < chunk; ++t) {
@@ -884,24 +917,19 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
             CK(cudaStreamEndCapture(ctx->st, &g));
             CK(cudaGraphInstantiate(&ge.exec, g, 0));
             cudaGraphDestroy(g);
+            ge.kernels = launches_issued() - k0;
+            ctx->captured += ge.kernels;
             it = ctx->graphs.emplace(key, ge).first;
         }
         CK(cudaGraphLaunch(it->second.exec, ctx->st));
+        ctx->replayed += it->second.kernels;
         // regrid / tail state after the chunk
         bool last_tail = false;
         for (int t = 0; t < chunk; ++t) {
             const bool regrid = ((phase + t + 1) % R) == 0;
             last_tail = regrid || (final_chunk && t == chunk - 1);
         }
-        if (ctx->prof) {
-            CK(cudaStreamSynchronize(ctx->st));
-            for (auto& pe : it->second.prof) {
-                float ms = 0;
-                cudaEventElapsedTime(&ms, pe.second.first, pe.second.second);
-                ctx->prof_ms[pe.first] += ms;
-                ctx->prof_n[pe.first] += 1;
-            }
-        }
+        if (ctx->prof) ctx->prof_pending = &it->second;
         ctx->stepcount += chunk;
         ctx->tail_done = last_tail;
         done += chunk;
@@ -937,11 +965,15 @@ int amrlbm_timer_stop(amrlbm_ctx* ctx, float* ms) {
     CK(cudaEventRecord(ctx->t1, ctx->st));
     CK(cudaEventSynchronize(ctx->t1));
     CK(cudaEventElapsedTime(ms, ctx->t0, ctx->t1));
+    CK(cudaStreamSynchronize(ctx->st));
+    harvest_profile(ctx);
     return device_error(ctx);
 }
 
 int amrlbm_profile_enable(amrlbm_ctx* ctx, int32_t enable) {
     if (!ctx) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    harvest_profile(ctx);
     ctx->prof = enable != 0;
     for (int k = 0; k < 4; ++k) {
         ctx->prof_ms[k] = 0;
@@ -954,6 +986,7 @@ int amrlbm_profile_read(amrlbm_ctx* ctx, int32_t kernel, double* total_ms, int64
                         int64_t* cells) {
     if (!ctx || kernel < 0 || kernel > 3) return AMRLBM_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->st));
+    harvest_profile(ctx);
     if (total_ms) *total_ms = ctx->prof_ms[kernel];
     if (launches) *launches = ctx->prof_n[kernel];
     if (cells) {
@@ -964,7 +997,7 @@ int amrlbm_profile_read(amrlbm_ctx* ctx, int32_t kernel, double* total_ms, int64
 }
 
 int64_t amrlbm_launch_count(const amrlbm_ctx* ctx) {
-    return ctx ? (int64_t)(launches_issued() - ctx->launches0) : 0;
+    return ctx ? (int64_t)(launches_issued() - ctx->launches0 - ctx->captured + ctx->replayed) : 0;
 }
 
 int amrlbm_flush_l2(amrlbm_ctx* ctx) {
@@ -991,10 +1024,10 @@ int upload_blocks(amrlbm_ctx* ctx, int n, const int* ids, const double* h, const
     const StageLayout L = stage_layout(ctx->prm.nx, ctx->prm.ny);
     const int mask = (h ? 1 : 0) | (g ? 2 : 0) | (C ? 4 : 0) | (P ? 8 : 0) | (Ux ? 16 : 0) |
                      (Uy ? 32 : 0);
-    std::vector<double> host((size_t)n * L.per, 0.0);
+    double* host = ctx->h_stage;
     const size_t hs = L.g - L.h, cs = L.P - L.C, ps = L.Ux - L.P;
     for (int i = 0; i < n; ++i) {
-        double* rec = host.data() + (size_t)i * L.per;
+        double* rec = host + (size_t)i * L.per;
         if (h) std::memcpy(rec + L.h, h + i * hs, hs * 8);
         if (g) std::memcpy(rec + L.g, g + i * hs, hs * 8);
         if (C) std::memcpy(rec + L.C, C + i * cs, cs * 8);
@@ -1002,13 +1035,13 @@ int upload_blocks(amrlbm_ctx* ctx, int n, const int* ids, const double* h, const
         if (Ux) std::memcpy(rec + L.Ux, Ux + i * ps, ps * 8);
         if (Uy) std::memcpy(rec + L.Uy, Uy + i * ps, ps * 8);
     }
-    CK(cudaMemcpyAsync(ctx->d_stage, host.data(), host.size() * 8, cudaMemcpyHostToDevice,
+    CK(cudaMemcpyAsync(ctx->d_stage, host, (size_t)n * L.per * 8, cudaMemcpyHostToDevice,
                        ctx->st));
     CK(cudaMemcpyAsync(ctx->d_ids, ids, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->st));
     k_transfer<<<ctx->lc.grid_leaves, 256, 0, ctx->st>>>(ctx->s, ctx->d_ids, n, ctx->d_stage, 0,
                                                          mask, L);
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(ctx->st));  // host buffer goes out of scope
+    CK(cudaStreamSynchronize(ctx->st));  // the staging buffer is reused by the next call
     return 0;
 }
 }  // namespace

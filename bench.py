@@ -1,0 +1,396 @@
+#!/usr/bin/env python3
+"""Throughput of the FP64 block-structured AMR two-phase LBM step on B200.
+
+Workload: the rising bubble on a 256x512-cell base grid of 16x16 blocks with 3
+refinement levels (finest-equivalent 2048x4096), R=128 at (1024,512), density
+ratio 1000, viscosity ratio 100, Eo=10, Mo=1e-5, W=4, a regrid every 10 time
+steps. Synthetic inputs: the analytic bubble of the reference's start-up,
+evolved W warm-up steps.
+
+One bench step = one regrid interval: 10 iterations of the Main_Loop body
+(Fill_Ghost_Cells_C2, collision, Fill_Ghost_Cells_hg, streaming,
+Macroscopic_Values_h/g, Fill_Ghost_Cells_C) with Refine_Derefine_Mesh after the
+10th, run by the C ABI (amrlbm_step) as one CUDA graph. The L2 cache is flushed
+between bench steps (outside the timed intervals).
+
+value    = leaf-cell updates of all ranks / slowest rank's device time (MLUPS)
+hbm_gbs  = value x 352 B (every population and macroscopic field read and
+           written once per update)
+e2e      = the same updates timed around upload of every leaf's fields from
+           host memory -> amrlbm_step -> download of every leaf's fields and
+           the diagnostics, all through the C ABI (wall clock)
+--impl reference: the oracle (a C++/OpenMP restatement of the reference's
+           Fortran, which cannot be compiled here) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "amr-lbm-openmp-2d_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "MLUPS and HBM GB/s on 1 B200: mixed-prec batched vs FP64 plain at stated error"
+BYTES_PER_UPDATE = 352  # 2 * (18 populations + C, P, Ux, Uy) * 8 B
+# algorithmic bytes per leaf cell of the fused kernels (reads + writes, FP64)
+KERNELS = {
+    0: ("fill_c2_collide", 296),        # h,g,C in; h,g out
+    1: ("fill_hg_stream_macro_h", 296), # h,g in; h,g,C out
+    2: ("fill_c_macro_g_err", 104),     # g,C in; P,Ux,Uy out
+    3: ("regrid", None),
+}
+WORKLOAD = "rising_bubble_base256x512_blocks16_L3_R128"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="own", choices=["own", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--max-blks", type=int, default=0,
+                    help="pool capacity (default: a fully refined tree); smaller pools "
+                         "keep profiler captures small")
+    return ap.parse_args()
+
+
+def workload():
+    import amrlbm
+    return amrlbm.workload_large()
+
+
+def config_dict(p, inner):
+    return {"workload": WORKLOAD, "base_grid": "256x512", "block": f"{p.nx}x{p.ny}",
+            "levels": p.max_levels, "finest_equivalent": "2048x4096", "radius": p.radius,
+            "density_ratio": round(p.rho_h / p.rho_l, 6), "viscosity_ratio": p.visc_ratio,
+            "eo": p.bo, "mo": 1e-5, "w": p.w, "regrid_every": p.regrid_every,
+            "time_steps_per_bench_step": inner, "l2": "flushed between bench steps",
+            "parallelism": "replicas"}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel_name):
+    """dram bytes per launch from a committed ncu summary, if one exists."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_name}.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch_full_workload:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region: the
+    sampler is started and its first sample awaited before the timed region,
+    and one more sample is awaited after it."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return [l for l in f.read().splitlines() if l.strip()]
+        except OSError:
+            return []
+
+    def start(self):
+        import tempfile
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.index)],
+                stdout=fd, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        os.close(fd)
+        t0 = time.time()
+        while self.proc and not self._lines() and time.time() - t0 < 5.0:
+            time.sleep(0.02)
+        self.n0 = len(self._lines())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t0 = time.time()
+        while len(self._lines()) <= self.n0 and time.time() - t0 < 2.0:
+            time.sleep(0.02)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        lines = self._lines()
+        os.unlink(self.path)
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(backend):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def allreduce(vals, op, world, device=None):
+    if world == 1:
+        return vals
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(vals, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op)
+    return t.tolist()
+
+
+def cpu_baseline_run(p, inner, seconds, max_chunks=400):
+    """The oracle on every host core: chunks of `inner` time steps until
+    `seconds` of CPU work (bounded sample of the same workload)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    threads = os.cpu_count() or 1
+    orc = Oracle(p, threads)
+    orc.initialize_rising_bubble()
+    updates, elapsed, chunks = 0, 0.0, 0
+    while elapsed < seconds and chunks < max_chunks:
+        nleaf = orc.counts()["nleaf"]
+        t = time.perf_counter()
+        orc.main_loop(inner)
+        elapsed += time.perf_counter() - t
+        updates += nleaf * p.nx * p.ny * inner  # the regrid is after the last step
+        chunks += 1
+    return updates / elapsed / 1e6, threads, chunks, elapsed
+
+
+def run_reference(args):
+    world, rank, local = dist_setup("gloo")
+    if rank != 0:
+        return 0
+    p = workload()
+    inner = p.regrid_every
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    threads = os.cpu_count() or 1
+    orc = Oracle(p, threads)
+    orc.initialize_rising_bubble()
+    for _ in range(args.warmup):
+        orc.main_loop(inner)
+    updates, total = 0, 0.0
+    for _ in range(args.steps):
+        nleaf = orc.counts()["nleaf"]
+        t = time.perf_counter()
+        orc.main_loop(inner)
+        total += time.perf_counter() - t
+        updates += nleaf * p.nx * p.ny * inner
+    v = updates / total / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(p, inner),
+            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} bench steps of {inner} time steps of "
+                                       f"the workload after {args.warmup} warm-up steps"},
+            "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_own(args):
+    world, rank, local = dist_setup("nccl")
+    import amrlbm
+    import numpy as np
+    dev = None
+    if world > 1:
+        import torch
+        torch.cuda.set_device(local)
+        dev = torch.device("cuda", local)
+    p = workload()
+    p.device = local
+    if args.max_blks:
+        p.max_blks = args.max_blks
+    inner = p.regrid_every
+    gpu = amrlbm.AmrLbm(p)
+    gpu.initialize_rising_bubble()
+    for _ in range(args.warmup):
+        gpu.main_loop(inner)
+    gpu.sync()
+
+    def barrier():
+        gpu.sync()
+        if world > 1:
+            import torch
+            import torch.distributed as dist
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    # ---- device-timed region
+    gpu.profile(True)
+    _, _, upd0 = gpu.profile_read(0)
+    launches0 = gpu.launch_count()
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        gpu.flush_l2()
+        gpu.sync()
+        gpu.timer_start()
+        gpu.main_loop(inner)
+        total_ms += gpu.timer_stop()
+    clk = clocks.stop()
+    barrier()
+    launches = gpu.launch_count() - launches0
+    kern = {}
+    for k, (name, bpc) in KERNELS.items():
+        ms, n, upd = gpu.profile_read(k)
+        kern[k] = (name, bpc, ms, n)
+    updates = upd - upd0
+    gpu.profile(False)
+    max_ms = allreduce([total_ms], _op("max"), world, dev)[0]
+    all_updates = allreduce([float(updates)], _op("sum"), world, dev)[0]
+    value = all_updates / (max_ms / 1e3) / 1e6
+
+    # ---- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        ids = gpu.leaves()
+        state = gpu.download_fields(ids)
+        _, _, u0 = gpu.profile_read(0)
+        h2d = d2h = 0
+        barrier()
+        t_e2e = 0.0
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            gpu.upload_fields(ids, state)
+            h2d += sum(a.nbytes for a in state.values()) + ids.nbytes
+            gpu.main_loop(inner)
+            ids = gpu.leaves()
+            state = gpu.download_fields(ids)
+            diag = gpu.output()
+            d2h += sum(a.nbytes for a in state.values()) + ids.nbytes + 8 * len(diag)
+            t_e2e += time.perf_counter() - t
+        barrier()
+        _, _, u1 = gpu.profile_read(0)
+        t_max = allreduce([t_e2e], _op("max"), world, dev)[0]
+        u_all = allreduce([float(u1 - u0)], _op("sum"), world, dev)[0]
+        e2e = {"value": u_all / t_max / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": int(h2d / args.steps),
+               "d2h_bytes_per_step": int(d2h / args.steps)}
+
+    diag = gpu.output()
+    if rank != 0:
+        gpu.close()
+        _finish(world)
+        return 0
+
+    # ---- roofline of the dominant kernel
+    peak, peak_kind = measured_peak()
+    dom = max((k for k in kern if kern[k][1]), key=lambda k: kern[k][2])
+    name, bpc, ms, n = kern[dom]
+    cells_per_launch = updates / max(kern[0][3], 1)  # every kernel visits every leaf
+    avg_s = ms / max(n, 1) / 1e3
+    achieved = cells_per_launch * bpc / avg_s / 1e9
+    traffic = profile_traffic(name)
+    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                               if peak_kind == "measured" else "fallback 6650 GB/s",
+                "algorithmic_bytes_per_cell": bpc, "cells_per_launch": cells_per_launch,
+                "avg_launch_us": avg_s * 1e6}
+    total_prof = sum(v[2] for v in kern.values()) or 1.0
+    kernels = {v[0]: {"launches": v[3], "total_ms": round(v[2], 4),
+                      "avg_us": round(v[2] / max(v[3], 1) * 1e3, 2),
+                      "share": round(v[2] / total_prof, 4)} for v in kern.values()}
+
+    cpu = None
+    if not args.no_cpu_baseline and world >= 1:
+        v, threads, chunks, el = cpu_baseline_run(workload(), inner, args.cpu_seconds)
+        cpu = {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port",
+               "sample": f"{chunks} x {inner} time steps of the same workload from its "
+                         f"start-up state ({el:.1f} s)"}
+    line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic rising bubble of the reference start-up)",
+            "config": config_dict(p, inner), "hbm_gbs": value * 1e6 * BYTES_PER_UPDATE / 1e9,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": int(launches), "kernels": kernels,
+            "leaf_cells_per_step": updates / max(kern[0][3], 1),
+            "diagnostics": {k: diag[k] for k in ("mass", "y_centroid", "rise_velocity")}}
+    print(json.dumps(line), flush=True)
+    gpu.close()
+    _finish(world)
+    return 0
+
+
+def _op(name):
+    try:
+        import torch.distributed as dist
+        return dist.ReduceOp.MAX if name == "max" else dist.ReduceOp.SUM
+    except Exception:
+        return None
+
+
+def _finish(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_own(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

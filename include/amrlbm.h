@@ -75,7 +75,7 @@ typedef struct amrlbm_params {
     int32_t max_levels;      /* maxLevels                                            */
     int32_t max_blks;        /* MaxBlks: pool capacity (blocks)                      */
     int32_t regrid_every;    /* regrid after every n-th step (reference: 1)          */
-    int32_t reserved0;
+    int32_t device;          /* CUDA device of the pool; < 0: the current device     */
     double rho_l, rho_h;     /* Rhol, Rhoh                                            */
     double visc_ratio;       /* muh/mul (reference: 100)                              */
     double bo, ar;           /* Bond (=Eotvos) and Archimedes numbers                 */
