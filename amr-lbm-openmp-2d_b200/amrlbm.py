@@ -199,6 +199,8 @@ def load_library(path: str | None = None):
                                            ct.POINTER(ct.c_int64)]),
         "amrlbm_launch_count": (ct.c_int64, [vp]),
         "amrlbm_flush_l2": (ct.c_int, [vp]),
+        "amrlbm_selftest_division": (ct.c_int, [ct.c_uint64, ct.c_uint64, ct.c_double,
+                                                ct.POINTER(ct.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

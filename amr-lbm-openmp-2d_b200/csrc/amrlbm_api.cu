@@ -98,6 +98,16 @@ PhysD to_physd(const amrlbm_physics& p) {
     d.Gy = p.gy;
     d.M0 = p.m0;
     d.wc = 1.0 / (0.5 + d.M0 * 3.0);  // D2Q9_Mod.f90:11
+    d.Beta4 = 4.0 * d.Beta;
+    d.omwc = 1.0 - d.wc;
+    d.dRho = d.Rhoh - d.Rhol;
+    d.dRho3 = (d.Rhoh - d.Rhol) / 3.0;
+    d.dRho6 = (d.Rhoh - d.Rhol) / 6.0;
+    d.itau_d = 1.0 / d.tauh - 1.0 / d.taul;
+    d.itaul = 1.0 / d.taul;
+    d.taul5 = d.taul + 0.5;
+    d.tauh5 = d.tauh + 0.5;
+    d.yW = 1.0 / d.W;
     return d;
 }
 
@@ -169,6 +179,10 @@ __global__ void k_transfer(DevState s, const int* ids, int n, double* stage, int
 
 int ensure_stage(amrlbm_ctx* ctx, size_t nblocks) {
     const StageLayout L = stage_layout(ctx->prm.nx, ctx->prm.ny);
+    // grow geometrically: the leaf count changes at every regrid
+    if (nblocks * L.per > ctx->stage_doubles || nblocks * L.per > ctx->h_stage_doubles)
+        nblocks = nblocks + nblocks / 2 + 16;
+    if (nblocks > (size_t)ctx->prm.max_blks) nblocks = (size_t)ctx->prm.max_blks;
     const size_t need = nblocks * L.per;
     if (need > ctx->stage_doubles) {
         if (ctx->d_stage) cudaFree(ctx->d_stage);
@@ -264,7 +278,8 @@ struct ProfMark {
     }
 };
 
-void enqueue_step(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail, bool regrid) {
+void enqueue_step(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail, bool regrid,
+                  bool last) {
     const DevState& s = ctx->s;
     {
         ProfMark m(ctx, ge, 0);
@@ -272,7 +287,7 @@ void enqueue_step(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail, bo
     }
     {
         ProfMark m(ctx, ge, 1);
-        launch_fill_hg_stream(s, ctx->lc, ctx->st);
+        launch_fill_hg_stream(s, ctx->lc, ctx->st, last ? 1 : 0);
     }
     if (tail) {
         ProfMark m(ctx, ge, 2);
@@ -377,6 +392,7 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
         p->max_blks < p->nbx * p->nby)
         return AMRLBM_ERR_ARG;
     if ((p->dx0 >> p->max_levels) < 1) return AMRLBM_ERR_ARG;  // dx stays an integer >= 1
+    if (p->dx0 & (p->dx0 - 1)) return AMRLBM_ERR_ARG;  // powers of two (L0/nx = 2**maxLevels)
     int dev = 0, cc = 0, sms = 0;
     if (p->device >= 0 && cudaSetDevice(p->device) != cudaSuccess) return AMRLBM_ERR_CUDA;
     if (cudaGetDevice(&dev) != cudaSuccess) return AMRLBM_ERR_CUDA;
@@ -438,6 +454,8 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     AL(deref, uint8_t, NB);
     AL(alloc, uint8_t, NB);
     AL(child_alloc, uint8_t, NB);
+    AL(ring_out, uint8_t, NB);
+    AL(ring_done, int, NQUEUES * NB);
     AL(leaf, int, NB);
     AL(lvl_leaf, int, NB);
     AL(lvl_off, int, AMR_MAXLV + 1);
@@ -853,7 +871,7 @@ int amrlbm_fill_ghost_c2(amrlbm_ctx* ctx) {
 int amrlbm_phase_field_step(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
     launch_collide(ctx->s, ctx->lc, ctx->st);
-    launch_fill_hg_stream(ctx->s, ctx->lc, ctx->st);
+    launch_fill_hg_stream(ctx->s, ctx->lc, ctx->st, 1);
     ctx->tail_done = false;
     return sync_check(ctx);
 }
@@ -910,7 +928,7 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
             for (int t = 0; t < chunk; ++t) {
                 const bool regrid = ((phase + t + 1) % R) == 0;
                 const bool tail = regrid || (final_chunk && t == chunk - 1);
-                enqueue_step(ctx, &ge, prev_tail, tail, regrid);
+                enqueue_step(ctx, &ge, prev_tail, tail, regrid, final_chunk && t == chunk - 1);
                 prev_tail = tail;
             }
             cudaGraph_t g;
@@ -998,6 +1016,14 @@ int amrlbm_profile_read(amrlbm_ctx* ctx, int32_t kernel, double* total_ms, int64
 
 int64_t amrlbm_launch_count(const amrlbm_ctx* ctx) {
     return ctx ? (int64_t)(launches_issued() - ctx->launches0 - ctx->captured + ctx->replayed) : 0;
+}
+
+int amrlbm_selftest_division(uint64_t n, uint64_t seed, double divisor, uint64_t* mismatches) {
+    if (!mismatches) return AMRLBM_ERR_ARG;
+    unsigned long long m = 0;
+    const int r = selftest_division(n, seed, divisor, &m);
+    *mismatches = m;
+    return r;
 }
 
 int amrlbm_flush_l2(amrlbm_ctx* ctx) {

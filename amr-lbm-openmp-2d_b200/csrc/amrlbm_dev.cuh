@@ -15,6 +15,17 @@
 // physical constants (D2Q9_Mod.f90:10-16)
 struct PhysD {
     double W, Sigma, Beta, kappa, taul, tauh, Rhol, Rhoh, Gy, M0, wc;
+    // constant sub-expressions of the reference's formulas, evaluated once on
+    // the host with the same operations (so the values are identical)
+    double Beta4;        // 4.d0*Beta                      (LBM_Subroutines.f90:108)
+    double omwc;         // 1.d0-wc                        (:146)
+    double dRho;         // Rhoh - Rhol                    (:150)
+    double dRho3;        // (Rhoh - Rhol)/3.d0             (:129)
+    double dRho6;        // (Rhoh-Rhol)/6.d0               (:216)
+    double itau_d;       // 1.d0/tauh - 1.d0/taul          (:174)
+    double itaul;        // 1.d0/taul                      (:174)
+    double taul5, tauh5; // taul + 0.5d0, tauh + 0.5d0     (:170-172)
+    double yW;           // RN(1/W)
 };
 
 // device counters of the block pool (Parameters.f90:6-10, 41-45)
@@ -56,6 +67,8 @@ struct DevState {
     int *gen;                                    // generation of each child array
     int *nbr;                                    // resolved neighbours [8*id + k-1]
     uint8_t *is_leaf, *has_leaf, *refin, *deref, *alloc, *child_alloc;
+    uint8_t* ring_out;  // leaf whose h/g ghost ring a finer neighbour reads
+    int* ring_done;     // [NQUEUES][max_blks+1]: ring written in the running fill
     int *leaf;       // LeafBlks, ascending
     int *lvl_leaf;   // leaves grouped by level (ascending level, then id)
     int *lvl_off;    // [AMR_MAXLV+1] offsets into lvl_leaf
@@ -81,9 +94,18 @@ __device__ __forceinline__ size_t p_idx(const DevState& s, int b, int x, int y) 
     return (size_t)b * s.pplane + (size_t)(y - 1) * s.nx + (x - 1);
 }
 
-// D2Q9 lattice (D2Q9_Mod.f90:6-8), 1-based
-__device__ __constant__ const int d_ex[10] = {0, 0, 1, 0, -1, 0, 1, -1, -1, 1};
-__device__ __constant__ const int d_ey[10] = {0, 0, 0, 1, 0, -1, 1, 1, -1, -1};
+// D2Q9 lattice (D2Q9_Mod.f90:6-8), 1-based:
+// ex = [0,1,0,-1,0,1,-1,-1,1], ey = [0,0,1,0,-1,1,1,-1,-1]. Functions, not a
+// __constant__ table, so that loops unrolled over k fold them into immediate
+// offsets and constants.
+__host__ __device__ __forceinline__ constexpr int cex(int k) {
+    return (k == 2 || k == 6 || k == 9) ? 1 : ((k == 4 || k == 7 || k == 8) ? -1 : 0);
+}
+__host__ __device__ __forceinline__ constexpr int cey(int k) {
+    return (k == 3 || k == 6 || k == 7) ? 1 : ((k == 5 || k == 8 || k == 9) ? -1 : 0);
+}
+#define d_ex(k) cex(k)
+#define d_ey(k) cey(k)
 
 __device__ __forceinline__ double wa(int i) {
     // [16,4,4,4,4,1,1,1,1]/36.d0, correctly rounded like the Fortran constant
@@ -118,7 +140,7 @@ __device__ __forceinline__ void gradient_ed(const double* E, double& Dx, double&
 template <class CF>
 __device__ __forceinline__ void ed_c(int dx, CF Cs, double* E) {
 #pragma unroll
-    for (int k = 1; k <= 9; ++k) E[k] = Cs(d_ex[k], d_ey[k]) - Cs(-d_ex[k], -d_ey[k]);
+    for (int k = 1; k <= 9; ++k) E[k] = Cs(d_ex(k), d_ey(k)) - Cs(-d_ex(k), -d_ey(k));
 #pragma unroll
     for (int k = 1; k <= 9; ++k) E[k] = E[k] * 0.5 / (double)dx;
 }
@@ -129,8 +151,8 @@ __device__ __forceinline__ void ed_m(int dx, CF Cs, double* E) {
     const double c0 = Cs(0, 0);
 #pragma unroll
     for (int k = 1; k <= 9; ++k)
-        E[k] = (-Cs(-d_ex[k], -d_ey[k]) - 3.0 * c0 + 5.0 * Cs(d_ex[k], d_ey[k]) -
-                Cs(2 * d_ex[k], 2 * d_ey[k]));
+        E[k] = (-Cs(-d_ex(k), -d_ey(k)) - 3.0 * c0 + 5.0 * Cs(d_ex(k), d_ey(k)) -
+                Cs(2 * d_ex(k), 2 * d_ey(k)));
 #pragma unroll
     for (int k = 1; k <= 9; ++k) E[k] = E[k] * 0.25 / (double)dx;
 }
@@ -149,8 +171,8 @@ __device__ __forceinline__ void equilibrium(const PhysD& ph, double C, double U,
     const double U2 = U * U + V * V;
 #pragma unroll
     for (int i = 1; i <= 9; ++i) {
-        const double eU = (double)d_ex[i] * U + (double)d_ey[i] * V;
-        const double eN = (double)d_ex[i] * ni + (double)d_ey[i] * nj;
+        const double eU = (double)d_ex(i) * U + (double)d_ey(i) * V;
+        const double eN = (double)d_ex(i) * ni + (double)d_ey(i) * nj;
         Gamma[i] = wa(i) * (1.0 + eU * (3.0 + 4.5 * eU) - 1.5 * U2);
         heq[i] = C * (Gamma[i] + tmp * wa(i) * eN);
     }
@@ -246,7 +268,7 @@ __device__ __forceinline__ void collide_cell(const PhysD& ph, int dx, CF Cs, dou
 #pragma unroll
         for (int k = 1; k <= 9; ++k)
             hlp[k] = ((Gamma[k] - wa(k)) * dRho3 + Gamma[k] * mu) * (E[k] - ud) +
-                     ((double)d_ey[k] - Uy) * Gamma[k] * Fb;
+                     ((double)d_ey(k) - Uy) * Gamma[k] * Fb;
     }
 #pragma unroll
     for (int k = 1; k <= 9; ++k) geq[k] = P * wa(k) + (Gamma[k] - wa(k)) * Rho / 3.0 - 0.5 * hlp[k];
@@ -257,7 +279,7 @@ __device__ __forceinline__ void collide_cell(const PhysD& ph, int dx, CF Cs, dou
 #pragma unroll
         for (int k = 1; k <= 9; ++k)
             hlp[k] = ((Gamma[k] - wa(k)) * dRho3 + Gamma[k] * mu) * (E[k] - ud) +
-                     ((double)d_ey[k] - Uy) * Gamma[k] * Fb;
+                     ((double)d_ey(k) - Uy) * Gamma[k] * Fb;
     }
     double tau;
     if (Cij < 0.0) {

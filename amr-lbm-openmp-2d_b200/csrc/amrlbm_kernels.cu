@@ -1,16 +1,10 @@
 // amrlbm_kernels.cu - FP64 sm_100a kernels of the block-structured AMR
-// two-phase lattice Boltzmann step. Compiled with -fmad=false: every FP64
-// operation is rounded separately, in the reference's order.
+// two-phase lattice Boltzmann path that run outside the time step: start-up
+// fields, the regrid (flags, 2:1 balance, derefine with restriction, refine
+// with neighbour pointers and prolongation, leaf lists) and diagnostics.
+// Compiled with -fmad=false: every FP64 operation is rounded separately, in
+// the reference's order. The per-step kernels are in amrlbm_step.cu.
 //
-// Level-ordered launches. The reference fills ghost cells level by level
-// (Fill_Ghost_Cells_C.f90:8-38): a coarse-to-fine fill reads the coarse
-// neighbour's ghost ring, which the previous level wrote. Here one launch
-// serves all levels: CTAs claim leaves from a queue sorted by level; a leaf
-// of level L waits (bounded spin) until every leaf of a coarser level has
-// published its ring. A waited-on leaf was claimed earlier by a running CTA,
-// so the wait always ends. After its fill a CTA goes on with the work that
-// only needs its own ring (collision, streaming, macroscopic values), so one
-// launch does "fill + consumer" with no grid-wide barrier.
 #include <cstdio>
 
 #include "amrlbm_launch.h"
@@ -19,244 +13,14 @@ namespace {
 
 long long g_launches = 0;
 
-constexpr int kSpinLimit = 20000000;  // x ~64 ns: about a second
-
-__device__ __forceinline__ int ld_acquire(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return (int)v;
-}
-
-// Claims the next item of queue q; returns its index (block-uniform).
-__device__ __forceinline__ int claim(const DevState& s, int q, int* slot) {
-    __syncthreads();
-    if (threadIdx.x == 0) *slot = (int)atomicAdd(&s.queue[2 * q], 1u);
-    __syncthreads();
-    return *slot;
-}
-
-// Waits until `target` items of queue q are done (thread 0 spins).
-__device__ __forceinline__ void wait_done(const DevState& s, int q, int target) {
-    if (threadIdx.x == 0 && target > 0) {
-        int it = 0;
-        while (ld_acquire(&s.queue[2 * q + 1]) < target) {
-            if (++it > kSpinLimit) {
-                set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, q);
-                break;
-            }
-            __nanosleep(64);
-        }
-    }
+__device__ __forceinline__ void load_tile(const DevState& s, int n, double* T) {
+    const int nx = s.nx, ny = s.ny, W = nx + 4, H = ny + 4;
+    for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x)
+        T[idx] = s.C[c_idx(s, n, idx % W - 1, idx / W - 1)];
     __syncthreads();
 }
 
-__device__ __forceinline__ void publish_done(const DevState& s, int q) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(&s.queue[2 * q + 1], 1u);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Fill_Ghost_Cells_C / _C2: value of ghost cell (x,y) of block n (level L)
-// from its direction-d neighbour N. Returns 1 if written, -1 on a level jump.
-// The gathers and stencils mirror Fill_Left_C .. Fill_Right_Top_C
-// (Fill_Ghost_Cells_C.f90:44-416, _C2.f90:44-416) case by case.
-__device__ int fill_c_value(const DevState& s, int n, int L, int N, int d, int x, int y,
-                            double& v) {
-    const int nx = s.nx, ny = s.ny;
-    const int Ln = s.level[N];
-    const bool left = (d == 1 || d == 5 || d == 6), right = (d == 2 || d == 7 || d == 8);
-    const bool bottom = (d == 3 || d == 5 || d == 7), top = (d == 4 || d == 6 || d == 8);
-    const int a = left ? 1 - x : (right ? x - nx : 0);  // layer counted outward
-    const int b = bottom ? 1 - y : (top ? y - ny : 0);
-    const double* C = s.C;
-    if (L == Ln) {
-        if (s.is_leaf[N]) {  // same-level leaf: copy
-            const int sx = left ? nx + 1 - a : (right ? a : x);
-            const int sy = bottom ? ny + 1 - b : (top ? b : y);
-            v = ldcg(&C[c_idx(s, N, sx, sy)]);
-            return 1;
-        }
-        const int c1 = s.child[4 * N];  // same-level parent: Biquadratic_from_Fine
-        if (d == 1 || d == 2) {
-            v = biq_fine_pt(a, y, [&](int r, int J) {
-                const int ch = (J <= ny) ? (d == 1 ? c1 + 1 : c1) : (d == 1 ? c1 + 3 : c1 + 2);
-                const int jj = (J <= ny) ? J : J - ny;
-                const int xx = (d == 1) ? nx - r + 1 : r;
-                return ldcg(&C[c_idx(s, ch, xx, jj)]);
-            });
-        } else if (d == 3 || d == 4) {
-            v = biq_fine_pt(x, b, [&](int I, int r) {
-                const int ch = (I <= nx) ? (d == 3 ? c1 + 2 : c1) : (d == 3 ? c1 + 3 : c1 + 1);
-                const int ii = (I <= nx) ? I : I - nx;
-                const int yy = (d == 3) ? ny - r + 1 : r;
-                return ldcg(&C[c_idx(s, ch, ii, yy)]);
-            });
-        } else {
-            const int ch = c1 + (d == 5 ? 3 : d == 6 ? 1 : d == 7 ? 2 : 0);
-            v = biq_fine_pt(a, b, [&](int k, int l) {
-                const int xx = left ? nx - k + 1 : k;
-                const int yy = bottom ? ny - l + 1 : l;
-                return ldcg(&C[c_idx(s, ch, xx, yy)]);
-            });
-        }
-        return 1;
-    }
-    if (L == Ln + 1) {  // coarser neighbour: Biquadratic_from_Coarse
-        if (d == 1 || d == 2) {
-            const int Y = (ny / 2) * (s.bj[n] % 2);
-            v = biq_coarse_pt(a, y, [&](int ii, int jj) {
-                const int xx = (d == 1) ? nx + 2 - ii : ii - 1;
-                return ldcg(&C[c_idx(s, N, xx, jj - 1 + Y)]);
-            });
-        } else if (d == 3 || d == 4) {
-            const int X = (nx / 2) * (s.bi[n] % 2);
-            v = biq_coarse_pt(x, b, [&](int ii, int jj) {
-                const int yy = (d == 3) ? ny + 2 - jj : jj - 1;
-                return ldcg(&C[c_idx(s, N, ii - 1 + X, yy)]);
-            });
-        } else {
-            const int mi = s.bi[n] % 2, mj = s.bj[n] % 2;
-            const int I = left ? nx - (nx / 2) * mi - 1 : nx / 2 - (nx / 2) * mi;
-            const int J = bottom ? ny - (ny / 2) * mj - 1 : ny / 2 - (ny / 2) * mj;
-            v = biq_coarse_pt(a, b, [&](int ii, int jj) {
-                const int xx = left ? I + 3 - ii : I + ii - 1;
-                const int yy = bottom ? J + 3 - jj : J + jj - 1;
-                return ldcg(&C[c_idx(s, N, xx, yy)]);
-            });
-        }
-        return 1;
-    }
-    return -1;
-}
-
-// direction (1..8) of ghost cell (x,y)
-__device__ __forceinline__ int ghost_dir(int x, int y, int nx, int ny) {
-    const bool xl = x < 1, xr = x > nx, yb = y < 1, yt = y > ny;
-    if (xl) return yb ? 5 : (yt ? 6 : 1);
-    if (xr) return yb ? 7 : (yt ? 8 : 2);
-    return yb ? 3 : 4;
-}
-
-// Fills the C ring of width w of block n into global memory and into the
-// shared tile T ((nx+4) x (ny+4), index (y+1)*(nx+4)+(x+1)); the interior of
-// T must already be loaded. Ends with the ring complete in T and in memory.
-__device__ void fill_c_block(const DevState& s, int n, int L, const int* nb, int w,
-                             double* T) {
-    const int nx = s.nx, ny = s.ny, TW = nx + 4;
-    const int W = nx + 2 * w, H = ny + 2 * w;
-    for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x) {
-        const int x = idx % W - w + 1, y = idx / W - w + 1;
-        if (x >= 1 && x <= nx && y >= 1 && y <= ny) continue;
-        const int d = ghost_dir(x, y, nx, ny);
-        const int N = nb[d];
-        if (N <= 0) continue;
-        double v;
-        const int r = fill_c_value(s, n, L, N, d, x, y, v);
-        if (r < 0) {
-            set_error(s, 4 /*AMRLBM_ERR_LEVEL_JUMP*/, n);
-            continue;
-        }
-        s.C[c_idx(s, n, x, y)] = v;
-        T[(y + 1) * TW + (x + 1)] = v;
-    }
-    __syncthreads();
-    // Symmetric_C(2)_3/4 (BC_Cell.f90:46-104): overwrite the wall rows
-    if (nb[3] < 0) {
-        for (int X = threadIdx.x - (w - 1); X <= nx + w; X += blockDim.x) {
-            if (X < 1 - w) continue;
-            for (int a = 1; a <= w; ++a) {  // C(X,1-a) = C(X,a)
-                const double v = T[(a + 1) * TW + (X + 1)];
-                T[(1 - a + 1) * TW + (X + 1)] = v;
-                s.C[c_idx(s, n, X, 1 - a)] = v;
-            }
-        }
-    }
-    if (nb[4] < 0) {
-        for (int X = threadIdx.x - (w - 1); X <= nx + w; X += blockDim.x) {
-            if (X < 1 - w) continue;
-            for (int a = 1; a <= w; ++a) {  // C(X,ny+a) = C(X,ny+1-a)
-                const double v = T[(ny + 1 - a + 1) * TW + (X + 1)];
-                T[(ny + a + 1) * TW + (X + 1)] = v;
-                s.C[c_idx(s, n, X, ny + a)] = v;
-            }
-        }
-    }
-    __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
-// Fill_Ghost_Cells_hg (Fill_Ghost_Cells_hg.f90:53-477): ghost cell (x,y) of
-// population q of the post-collision field A.
-__device__ int fill_hg_value(const DevState& s, const double* A, int n, int L, int N, int d,
-                             int q, int x, int y, double& v) {
-    const int nx = s.nx, ny = s.ny;
-    const int Ln = s.level[N];
-    const bool left = (d == 1 || d == 5 || d == 6), right = (d == 2 || d == 7 || d == 8);
-    const bool bottom = (d == 3 || d == 5 || d == 7), top = (d == 4 || d == 6 || d == 8);
-    if (L == Ln) {
-        if (s.is_leaf[N]) {
-            const int sx = left ? nx : (right ? 1 : x);
-            const int sy = bottom ? ny : (top ? 1 : y);
-            v = ldcg(&A[a_idx(s, N, q, sx, sy)]);
-            return 1;
-        }
-        const int c1 = s.child[4 * N];
-        if (d == 1 || d == 2) {
-            v = biq_fine_pt(1, y, [&](int r, int J) {
-                const int ch = (J <= ny) ? (d == 1 ? c1 + 1 : c1) : (d == 1 ? c1 + 3 : c1 + 2);
-                const int jj = (J <= ny) ? J : J - ny;
-                const int xx = (d == 1) ? nx - r + 1 : r;
-                return ldcg(&A[a_idx(s, ch, q, xx, jj)]);
-            });
-        } else if (d == 3 || d == 4) {
-            v = biq_fine_pt(x, 1, [&](int I, int r) {
-                const int ch = (I <= nx) ? (d == 3 ? c1 + 2 : c1) : (d == 3 ? c1 + 3 : c1 + 1);
-                const int ii = (I <= nx) ? I : I - nx;
-                const int yy = (d == 3) ? ny - r + 1 : r;
-                return ldcg(&A[a_idx(s, ch, q, ii, yy)]);
-            });
-        } else {
-            const int ch = c1 + (d == 5 ? 3 : d == 6 ? 1 : d == 7 ? 2 : 0);
-            v = biq_fine_pt(1, 1, [&](int k, int l) {
-                const int xx = left ? nx - k + 1 : k;
-                const int yy = bottom ? ny - l + 1 : l;
-                return ldcg(&A[a_idx(s, ch, q, xx, yy)]);
-            });
-        }
-        return 1;
-    }
-    if (L == Ln + 1) {
-        if (d == 1 || d == 2) {
-            const int Y = (ny / 2) * (s.bj[n] % 2);
-            v = biq_coarse_pt(1, y, [&](int ii, int jj) {
-                const int xx = (d == 1) ? nx + 2 - ii : ii - 1;
-                return ldcg(&A[a_idx(s, N, q, xx, jj - 1 + Y)]);
-            });
-        } else if (d == 3 || d == 4) {
-            const int X = (nx / 2) * (s.bi[n] % 2);
-            v = biq_coarse_pt(x, 1, [&](int ii, int jj) {
-                const int yy = (d == 3) ? ny + 2 - jj : jj - 1;
-                return ldcg(&A[a_idx(s, N, q, ii - 1 + X, yy)]);
-            });
-        } else {
-            const int mi = s.bi[n] % 2, mj = s.bj[n] % 2;
-            const int I = left ? nx - (nx / 2) * mi - 1 : nx / 2 - (nx / 2) * mi;
-            const int J = bottom ? ny - (ny / 2) * mj - 1 : ny / 2 - (ny / 2) * mj;
-            v = biq_coarse_pt(1, 1, [&](int ii, int jj) {
-                const int xx = left ? I + 3 - ii : I + ii - 1;
-                const int yy = bottom ? J + 3 - jj : J + jj - 1;
-                return ldcg(&A[a_idx(s, N, q, xx, yy)]);
-            });
-        }
-        return 1;
-    }
-    return -1;
-}
-
-// ring cell index r in [0, 2(nx+ny)+4) -> (x,y) of ring 1
+// ring 1 of a block: index r in [0, 2(nx+ny)+4) -> (x,y)
 __device__ __forceinline__ void ring1_xy(int r, int nx, int ny, int& x, int& y) {
     if (r < nx + 2) {
         x = r;
@@ -268,293 +32,6 @@ __device__ __forceinline__ void ring1_xy(int r, int nx, int ny, int& x, int& y) 
         const int t = r - 2 * (nx + 2);
         x = (t < ny) ? 0 : nx + 1;
         y = 1 + (t < ny ? t : t - ny);
-    }
-}
-
-// Fills ring 1 of h and g (post-collision A arrays) of block n, then applies
-// Bounce_Back_3/4 (BC_Cell.f90:2-42).
-__device__ void fill_hg_block(const DevState& s, int n, int L, const int* nb) {
-    const int nx = s.nx, ny = s.ny;
-    const int R = 2 * (nx + ny) + 4;
-    for (int idx = threadIdx.x; idx < R * 18; idx += blockDim.x) {
-        const int r = idx % R, qf = idx / R;
-        const int q = qf % 9 + 1;
-        double* A = (qf < 9) ? s.Ah : s.Ag;
-        int x, y;
-        ring1_xy(r, nx, ny, x, y);
-        const int d = ghost_dir(x, y, nx, ny);
-        const int N = nb[d];
-        if (N <= 0) continue;
-        double v;
-        if (fill_hg_value(s, A, n, L, N, d, q, x, y, v) < 0) {
-            set_error(s, 4, n);
-            continue;
-        }
-        A[a_idx(s, n, q, x, y)] = v;
-    }
-    __syncthreads();
-    for (int wall = 3; wall <= 4; ++wall) {
-        if (nb[wall] >= 0) continue;
-        const int Y = (wall == 3) ? 0 : ny + 1, Yi = (wall == 3) ? 1 : ny;
-        const int sgn = (wall == 3) ? 1 : -1;
-        for (int idx = threadIdx.x; idx < (nx + 2) * 18; idx += blockDim.x) {
-            const int X = idx % (nx + 2), qf = idx / (nx + 2);
-            const int i = qf % 9 + 1;
-            double* A = (qf < 9) ? s.Ah : s.Ag;
-            double v;
-            if (i == 1) {
-                v = A[a_idx(s, n, 1, X, Yi)];
-            } else {
-                int Xn = X + sgn * d_ex[i] * d_ey[i];
-                Xn = min(max(0, Xn), nx + 1);
-                const int J = (i - 2) + 4 * ((i / 2) % 2);
-                v = A[a_idx(s, n, J, Xn, Yi)];
-            }
-            A[a_idx(s, n, i, X, Y)] = v;
-        }
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// collision of one cell of block n from the shared C tile T
-template <int CONSUMER>
-__device__ __forceinline__ void collide_consumer(const DevState& s, int n, const double* T) {
-    const int nx = s.nx, ny = s.ny, TW = nx + 4;
-    const int dx = s.dx[n];
-    for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
-        const int x = c % nx + 1, y = c / nx + 1;
-        auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 1) * TW + (x + ddx + 1)]; };
-        double h[10], g[10];
-#pragma unroll
-        for (int q = 1; q <= 9; ++q) {
-            h[q] = s.Bh[b_idx(s, n, q, x, y)];
-            g[q] = s.Bg[b_idx(s, n, q, x, y)];
-        }
-        double P, Ux, Uy;
-        if (CONSUMER == CONS_COLLIDE_FUSED) {
-            macro_g_cell(s.ph, dx, Cs, g, P, Ux, Uy);
-        } else {
-            P = s.P[p_idx(s, n, x, y)];
-            Ux = s.Ux[p_idx(s, n, x, y)];
-            Uy = s.Uy[p_idx(s, n, x, y)];
-        }
-        collide_cell(s.ph, dx, Cs, P, Ux, Uy, h, g);
-#pragma unroll
-        for (int q = 1; q <= 9; ++q) {
-            s.Ah[a_idx(s, n, q, x, y)] = h[q];
-            s.Ag[a_idx(s, n, q, x, y)] = g[q];
-        }
-    }
-}
-
-// Macroscopic_Values_g_AMR + Err_Interface of block n from the tile T
-__device__ void macro_g_err_consumer(const DevState& s, int n, const double* T, double* red) {
-    const int nx = s.nx, ny = s.ny, TW = nx + 4;
-    const int dx = s.dx[n];
-    double mx = 0.0;
-    for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
-        const int x = c % nx + 1, y = c / nx + 1;
-        auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 1) * TW + (x + ddx + 1)]; };
-        double g[10];
-#pragma unroll
-        for (int q = 1; q <= 9; ++q) g[q] = s.Bg[b_idx(s, n, q, x, y)];
-        double P, Ux, Uy;
-        macro_g_cell(s.ph, dx, Cs, g, P, Ux, Uy);
-        s.P[p_idx(s, n, x, y)] = P;
-        s.Ux[p_idx(s, n, x, y)] = Ux;
-        s.Uy[p_idx(s, n, x, y)] = Uy;
-        const double a = Cs(1, 0) - Cs(-1, 0), b = Cs(0, 1) - Cs(0, -1);
-        mx = fmax(mx, a * a + b * b);
-    }
-    // block max; fmax drops NaN like MAX(err, DC) with a NaN DC never chosen
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double m = 0.0;
-        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) m = fmax(m, red[w]);
-        s.err[n] = sqrt(m) / (2.0 * dx);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Level-ordered C ghost fill (+ consumer). Items: all leaves grouped by
-// level; leaves of levels outside [LevelMin, LevelMax] are not filled (as the
-// reference's DO L = LevelMin, LevelMax) but still get the consumer work.
-template <int CONSUMER>
-__global__ void __launch_bounds__(256) k_fill_c(DevState s, int w, int q) {
-    extern __shared__ double sm[];
-    double* T = sm;
-    double* red = sm + (s.nx + 4) * (s.ny + 4);
-    __shared__ int s_item, s_nb[9];
-    const int nx = s.nx, ny = s.ny, TW = nx + 4;
-    const int lmin = s.cnt->level_min, lmax = s.cnt->level_max;
-    const int total = s.lvl_off[AMR_MAXLV];
-    if (CONSUMER == CONS_COLLIDE_READ || CONSUMER == CONS_COLLIDE_FUSED)
-        if (blockIdx.x == 0 && threadIdx.x == 0)
-            atomicAdd(&s.cnt->updates, (unsigned long long)total * (unsigned long long)(nx * ny));
-    for (;;) {
-        const int k = claim(s, q, &s_item);
-        if (k >= total) break;
-        const int n = s.lvl_leaf[k];
-        const int L = s.level[n];
-        if (threadIdx.x < 8) s_nb[threadIdx.x + 1] = s.nbr[8 * n + threadIdx.x];
-        // the whole tile from memory; the fill overwrites the ring cells it owns
-        {
-            const int W = nx + 4, H = ny + 4;
-            for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x)
-                T[idx] = ldcg(&s.C[c_idx(s, n, idx % W - 1, idx / W - 1)]);
-        }
-        const bool do_fill = (L >= lmin && L <= lmax);
-        if (do_fill) {
-            wait_done(s, q, (L > 0) ? s.lvl_off[L] : 0);
-            fill_c_block(s, n, L, s_nb, w, T);
-        } else {
-            __syncthreads();
-        }
-        publish_done(s, q);
-        if (CONSUMER != CONS_NONE) {
-            __syncthreads();
-            if (CONSUMER == CONS_MACRO_G)
-                macro_g_err_consumer(s, n, T, red);
-            else
-                collide_consumer<CONSUMER>(s, n, T);
-        }
-    }
-    (void)TW;
-}
-
-// Level-ordered Fill_Ghost_Cells_hg + streaming (Perfect_Shift_AMR or
-// Streaming_LaxWendroff_AMR, LBM_Subroutines.f90:41-90) from A into B +
-// Macroscopic_Values_h_AMR (:193-201).
-__global__ void __launch_bounds__(256) k_fill_hg_stream(DevState s) {
-    __shared__ int s_item, s_nb[9];
-    const int nx = s.nx, ny = s.ny;
-    const int q = Q_FILLHG;
-    const int lmin = s.cnt->level_min, lmax = s.cnt->level_max;
-    const int total = s.lvl_off[AMR_MAXLV];
-    for (;;) {
-        const int k = claim(s, q, &s_item);
-        if (k >= total) break;
-        const int n = s.lvl_leaf[k];
-        const int L = s.level[n];
-        if (threadIdx.x < 8) s_nb[threadIdx.x + 1] = s.nbr[8 * n + threadIdx.x];
-        __syncthreads();
-        const bool do_fill = (L >= lmin && L <= lmax);
-        if (do_fill) {
-            wait_done(s, q, (L > 0) ? s.lvl_off[L] : 0);
-            fill_hg_block(s, n, L, s_nb);
-        }
-        publish_done(s, q);
-        __syncthreads();
-        const int dx = s.dx[n];
-        const double cfl = 1.0 / (double)dx;
-        const bool shift = cfl > (double)0.9f;
-        const double cA = cfl / 2.0 * (1.0 + cfl), cB = 1.0 - cfl * cfl, cC = cfl / 2.0 * (1.0 - cfl);
-        for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
-            const int x = c % nx + 1, y = c / nx + 1;
-            double csum = 0.0;
-#pragma unroll
-            for (int f = 0; f < 2; ++f) {
-                const double* A = f ? s.Ag : s.Ah;
-                double* B = f ? s.Bg : s.Bh;
-#pragma unroll
-                for (int i = 1; i <= 9; ++i) {
-                    double v;
-                    if (i == 1) {
-                        v = A[a_idx(s, n, 1, x, y)];
-                    } else if (shift) {
-                        v = A[a_idx(s, n, i, x - d_ex[i], y - d_ey[i])];
-                    } else {
-                        v = cA * A[a_idx(s, n, i, x - d_ex[i], y - d_ey[i])] +
-                            cB * A[a_idx(s, n, i, x, y)] -
-                            cC * A[a_idx(s, n, i, x + d_ex[i], y + d_ey[i])];
-                    }
-                    B[b_idx(s, n, i, x, y)] = v;
-                    if (f == 0) csum = csum + v;
-                }
-            }
-            s.C[c_idx(s, n, x, y)] = csum;
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// grid-stride kernels over the leaf list (one CTA per block)
-
-__device__ __forceinline__ void load_tile(const DevState& s, int n, double* T) {
-    const int nx = s.nx, ny = s.ny, W = nx + 4, H = ny + 4;
-    for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x) {
-        const int x = idx % W - 1, y = idx / W - 1;
-        T[idx] = s.C[c_idx(s, n, x, y)];
-    }
-    __syncthreads();
-}
-
-__global__ void __launch_bounds__(256) k_collide(DevState s) {
-    extern __shared__ double T[];
-    const int nleaf = s.cnt->nleaf;
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        atomicAdd(&s.cnt->updates, (unsigned long long)nleaf * (unsigned long long)(s.nx * s.ny));
-    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
-        const int n = s.leaf[m];
-        load_tile(s, n, T);
-        collide_consumer<CONS_COLLIDE_READ>(s, n, T);
-        __syncthreads();
-    }
-}
-
-__global__ void __launch_bounds__(256) k_macro_g(DevState s) {
-    extern __shared__ double sm[];
-    double* T = sm;
-    double* red = sm + (s.nx + 4) * (s.ny + 4);
-    const int nleaf = s.cnt->nleaf;
-    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
-        const int n = s.leaf[m];
-        load_tile(s, n, T);
-        macro_g_err_consumer(s, n, T, red);
-        __syncthreads();
-    }
-}
-
-// Macroscopic_Values_h_AMR (LBM_Subroutines.f90:193-201)
-__global__ void k_macro_h(DevState s) {
-    const int nleaf = s.cnt->nleaf, nn = s.nx * s.ny;
-    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
-        const int n = s.leaf[m];
-        for (int c = threadIdx.x; c < nn; c += blockDim.x) {
-            const int x = c % s.nx + 1, y = c / s.nx + 1;
-            double sum = 0.0;
-#pragma unroll
-            for (int q = 1; q <= 9; ++q) sum = sum + s.Bh[b_idx(s, n, q, x, y)];
-            s.C[c_idx(s, n, x, y)] = sum;
-        }
-    }
-}
-
-// Err_Interface (Refine_Derefine.f90:327-351) of every leaf
-__global__ void k_err(DevState s) {
-    __shared__ double red[32];
-    const int nleaf = s.cnt->nleaf, nx = s.nx, ny = s.ny;
-    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
-        const int n = s.leaf[m];
-        double mx = 0.0;
-        for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
-            const int x = c % nx + 1, y = c / nx + 1;
-            const double a = s.C[c_idx(s, n, x + 1, y)] - s.C[c_idx(s, n, x - 1, y)];
-            const double b = s.C[c_idx(s, n, x, y + 1)] - s.C[c_idx(s, n, x, y - 1)];
-            mx = fmax(mx, a * a + b * b);
-        }
-        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double r = 0.0;
-            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) r = fmax(r, red[w]);
-            s.err[n] = sqrt(r) / (2.0 * s.dx[n]);
-        }
-        __syncthreads();
     }
 }
 
@@ -590,7 +67,7 @@ __global__ void __launch_bounds__(256) k_init_fields(DevState s, double R) {
             for (int k = 1; k <= 9; ++k) {
                 s.Bh[b_idx(s, n, k, x, y)] = heq[k];
                 const double hlp = ((Gamma[k] - wa(k)) * dRho3 + Gamma[k] * mu) * (E[k] - ud) +
-                                   ((double)d_ey[k] - Uy) * Gamma[k] * Fb;
+                                   ((double)d_ey(k) - Uy) * Gamma[k] * Fb;
                 s.Bg[b_idx(s, n, k, x, y)] = P * wa(k) + (Gamma[k] - wa(k)) * Rho / 3.0 - 0.5 * hlp;
             }
         }
@@ -974,6 +451,16 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_topo(DevState s, i
     for (int m = threadIdx.x; m < nleaf; m += blockDim.x) {
         const int n = s.leaf[m];
         for (int k = 1; k <= 8; ++k) s.nbr[8 * n + k - 1] = resolve_chk(s, n, k);
+        s.ring_out[n] = 0;
+    }
+    __syncthreads();
+    // leaves whose h/g ghost ring a finer neighbour's coarse-to-fine fill reads
+    for (int m = threadIdx.x; m < nleaf; m += blockDim.x) {
+        const int n = s.leaf[m];
+        for (int k = 0; k < 8; ++k) {
+            const int b = s.nbr[8 * n + k];
+            if (b > 0 && s.level[b] == s.level[n] - 1) s.ring_out[b] = 1;
+        }
     }
 }
 
@@ -1182,7 +669,7 @@ __global__ void k_diag_final(DevState s, const double* part, double* out) {
 
 size_t tile_bytes(const DevState& s) { return (size_t)(s.nx + 4) * (s.ny + 4) * sizeof(double); }
 int block_threads(const DevState& s) {
-    const int t = ((s.nx * s.ny + 31) / 32) * 32;  // whole warps (shuffle reductions)
+    const int t = ((s.nx * s.ny + 31) / 32) * 32;
     return t > 256 ? 256 : t;
 }
 
@@ -1191,95 +678,57 @@ int block_threads(const DevState& s) {
 // ---------------------------------------------------------------------------
 // launchers
 long long launches_issued() { return g_launches; }
+void count_launches(int n) { g_launches += n; }
 
 void launch_reset_queues(const DevState& s, cudaStream_t st) {
     cudaMemsetAsync(s.queue, 0, sizeof(unsigned) * 2 * NQUEUES, st);
 }
 
-void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width,
-                   int consumer) {
-    const int q = (width == 2) ? Q_FILLC : Q_FILLC1;
-    cudaMemsetAsync(s.queue + 2 * q, 0, 2 * sizeof(unsigned), st);
-    const size_t sm = tile_bytes(s) + 32 * sizeof(double);
-    const int nt = block_threads(s);
-    switch (consumer) {
-        case CONS_NONE: k_fill_c<CONS_NONE><<<lc.grid_queue, nt, sm, st>>>(s, width, q); break;
-        case CONS_COLLIDE_READ:
-            k_fill_c<CONS_COLLIDE_READ><<<lc.grid_queue, nt, sm, st>>>(s, width, q);
-            break;
-        case CONS_COLLIDE_FUSED:
-            k_fill_c<CONS_COLLIDE_FUSED><<<lc.grid_queue, nt, sm, st>>>(s, width, q);
-            break;
-        default: k_fill_c<CONS_MACRO_G><<<lc.grid_queue, nt, sm, st>>>(s, width, q); break;
-    }
-    ++g_launches;
-}
 
-void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
-    cudaMemsetAsync(s.queue + 2 * Q_FILLHG, 0, 2 * sizeof(unsigned), st);
-    k_fill_hg_stream<<<lc.grid_queue, block_threads(s), 0, st>>>(s);
-    ++g_launches;
-}
 
-void launch_collide(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
-    k_collide<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s);
-    ++g_launches;
-}
 
-void launch_macro_h(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
-    k_macro_h<<<lc.grid_leaves, block_threads(s), 0, st>>>(s);
-    ++g_launches;
-}
 
-void launch_macro_g(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
-    k_macro_g<<<lc.grid_leaves, block_threads(s), tile_bytes(s) + 32 * sizeof(double), st>>>(s);
-    ++g_launches;
-}
 
-void launch_err(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
-    k_err<<<lc.grid_leaves, block_threads(s), 0, st>>>(s);
-    ++g_launches;
-}
 
 void launch_minmax(const DevState& s, cudaStream_t st) {
     k_minmax<<<1, 256, 0, st>>>(s);
-    ++g_launches;
+    count_launches(1);
 }
 
 void launch_init_fields(const DevState& s, const LaunchCfg& lc, cudaStream_t st, double radius) {
     k_init_fields<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s, radius);
-    ++g_launches;
+    count_launches(1);
 }
 
 void launch_regrid_flags(const DevState& s, cudaStream_t st, double refin_tol, double deref_tol) {
     k_regrid_flags<<<1, AMR_NTHREADS_TOPO, 0, st>>>(s, refin_tol, deref_tol);
-    ++g_launches;
+    count_launches(1);
 }
 
 void launch_restrict(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
     k_restrict<<<lc.grid_leaves, block_threads(s), 0, st>>>(s);
-    ++g_launches;
+    count_launches(1);
 }
 
 void launch_regrid_topo(const DevState& s, cudaStream_t st, int mode, int lmin, int lmax,
                         int set_levels) {
     k_regrid_topo<<<1, AMR_NTHREADS_TOPO, 0, st>>>(s, mode, lmin, lmax, set_levels);
-    ++g_launches;
+    count_launches(1);
 }
 
 void launch_prolong(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
     k_prolong<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s);
-    ++g_launches;
+    count_launches(1);
 }
 
 void launch_zero_children(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
     k_zero_children<<<lc.grid_leaves, 256, 0, st>>>(s);
-    ++g_launches;
+    count_launches(1);
 }
 
 void launch_flag_level(const DevState& s, cudaStream_t st, int level) {
     k_flag_level<<<64, 256, 0, st>>>(s, level);
-    ++g_launches;
+    count_launches(1);
 }
 
 void launch_diag(const DevState& s, cudaStream_t st, double* out9) {
@@ -1287,5 +736,5 @@ void launch_diag(const DevState& s, cudaStream_t st, double* out9) {
     double* part = out9 + 9;
     k_diag_blocks<<<64, 128, 0, st>>>(s, part);
     k_diag_final<<<1, 32, 0, st>>>(s, part, out9);
-    g_launches += 2;
+    count_launches(2);
 }

@@ -21,7 +21,8 @@ struct LaunchCfg {
 
 void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width,
                    int consumer);
-void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+// write_all: every ring goes to memory (else only rings a finer neighbour reads)
+void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int write_all);
 void launch_collide(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_macro_h(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_macro_g(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
@@ -43,3 +44,7 @@ void launch_diag(const DevState& s, cudaStream_t st, double* out8);
 void launch_reset_queues(const DevState& s, cudaStream_t st);
 // number of kernels the launchers above issued (for the launch counter)
 long long launches_issued();
+void count_launches(int n);
+// div_rn against IEEE division on n random operands (divisor 0: random)
+int selftest_division(unsigned long long n, unsigned long long seed, double divisor,
+                      unsigned long long* mismatches);

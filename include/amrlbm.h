@@ -214,6 +214,11 @@ int amrlbm_profile_read(amrlbm_ctx* ctx, int32_t kernel, double* total_ms,
                         int64_t* launches, int64_t* cells);
 /* Number of kernels this library launched since creation. */
 int64_t amrlbm_launch_count(const amrlbm_ctx* ctx);
+/* Self-test of the exact FP64 division used by the kernels (the FMA
+ * correction of Markstein's theorem, given a correctly rounded reciprocal)
+ * against IEEE division, on n random operands on the current device;
+ * divisor 0 draws random divisors. mismatches = results whose bits differ. */
+int amrlbm_selftest_division(uint64_t n, uint64_t seed, double divisor, uint64_t* mismatches);
 /* Writes a buffer larger than the L2 cache on the context's stream. */
 int amrlbm_flush_l2(amrlbm_ctx* ctx);
 
