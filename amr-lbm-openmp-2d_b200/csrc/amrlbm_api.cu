@@ -253,6 +253,7 @@ void enqueue_regrid(amrlbm_ctx* ctx, double rt, double dt, bool with_err, bool s
     launch_regrid_flags(s, ctx->st, rt, dt);
     launch_restrict(s, ctx->lc, ctx->st);
     launch_regrid_topo(s, ctx->st, 0, -1, -1, set_levels ? 1 : 0);
+    launch_build_plans(s, ctx->lc, ctx->st);
     launch_prolong(s, ctx->lc, ctx->st);
 }
 
@@ -287,7 +288,7 @@ void enqueue_step(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail, bo
     }
     {
         ProfMark m(ctx, ge, 1);
-        launch_fill_hg_stream(s, ctx->lc, ctx->st, last ? 1 : 0);
+        launch_fill_hg_stream(s, ctx->lc, ctx->st);
     }
     if (tail) {
         ProfMark m(ctx, ge, 2);
@@ -393,6 +394,11 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
         return AMRLBM_ERR_ARG;
     if ((p->dx0 >> p->max_levels) < 1) return AMRLBM_ERR_ARG;  // dx stays an integer >= 1
     if (p->dx0 & (p->dx0 - 1)) return AMRLBM_ERR_ARG;  // powers of two (L0/nx = 2**maxLevels)
+    {  // fill plans hold 32-bit offsets into the A pool
+        const size_t ap = ((size_t)p->nx + 5 + 3) / 4 * 4;
+        const size_t aplane = ((p->ny + 2) * ap + 15) / 16 * 16;
+        if (((size_t)p->max_blks + 1) * 9 * aplane >= (1ull << 32)) return AMRLBM_ERR_ARG;
+    }
     int dev = 0, cc = 0, sms = 0;
     if (p->device >= 0 && cudaSetDevice(p->device) != cudaSuccess) return AMRLBM_ERR_CUDA;
     if (cudaGetDevice(&dev) != cudaSuccess) return AMRLBM_ERR_CUDA;
@@ -459,6 +465,10 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     AL(leaf, int, NB);
     AL(lvl_leaf, int, NB);
     AL(lvl_off, int, AMR_MAXLV + 1);
+    AL(nbinfo, int, NB * NBI_STRIDE);
+    AL(plan_c2, int, NB * PLAN_INTS * (size_t)(4 * (nx + ny) + 16));
+    AL(plan_c1, int, NB * PLAN_INTS * (size_t)(2 * (nx + ny) + 4));
+    AL(plan_hg, int, NB * PLAN_INTS * (size_t)(2 * (nx + ny) + 4));
     AL(freelist, int, (size_t)s.fl_cap);
     AL(ref_list, int, NB);
     AL(ref_c1, int, NB);
@@ -607,6 +617,7 @@ int amrlbm_set_topology(amrlbm_ctx* ctx, int32_t nblks, const int32_t* level, co
     c.error = 0;
     CK(cudaMemcpyAsync(s.cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, ctx->st));
     launch_regrid_topo(s, ctx->st, 2, -1, -1, 0);
+    launch_build_plans(s, ctx->lc, ctx->st);
     ctx->tail_done = true;
     return sync_check(ctx);
 }
@@ -835,6 +846,7 @@ int amrlbm_init_rising_bubble(amrlbm_ctx* ctx) {
     for (int L = 1; L <= p.min_levels; ++L) {
         launch_flag_level(ctx->s, ctx->st, L - 1);
         launch_regrid_topo(ctx->s, ctx->st, 1, L - 1, L - 1, 0);
+        launch_build_plans(ctx->s, ctx->lc, ctx->st);
         launch_zero_children(ctx->s, ctx->lc, ctx->st);
     }
     if (int r = sync_check(ctx)) return r;
@@ -871,7 +883,7 @@ int amrlbm_fill_ghost_c2(amrlbm_ctx* ctx) {
 int amrlbm_phase_field_step(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
     launch_collide(ctx->s, ctx->lc, ctx->st);
-    launch_fill_hg_stream(ctx->s, ctx->lc, ctx->st, 1);
+    launch_fill_hg_stream(ctx->s, ctx->lc, ctx->st);
     ctx->tail_done = false;
     return sync_check(ctx);
 }

@@ -42,6 +42,10 @@ struct Counters {
 
 // Work queues of the level-ordered kernels: [2*q] = next item, [2*q+1] = items done.
 enum { Q_FILLC = 0, Q_FILLHG = 1, Q_FILLC1 = 2, NQUEUES = 3 };
+// per-leaf records of the level-ordered kernels, indexed by work-order
+// position: neighbour record (NBI_STRIDE ints) and one fill plan per ghost
+// cell (PLAN_INTS ints: kind/weights word + 9 source offsets)
+enum { NBI_STRIDE = 40, PLAN_INTS = 10 };
 
 // ---------------------------------------------------------------------------
 // The block pool. Block ids are 1..max_blks (slot 0 unused).
@@ -70,8 +74,10 @@ struct DevState {
     uint8_t* ring_out;  // leaf whose h/g ghost ring a finer neighbour reads
     int* ring_done;     // [NQUEUES][max_blks+1]: ring written in the running fill
     int *leaf;       // LeafBlks, ascending
-    int *lvl_leaf;   // leaves grouped by level (ascending level, then id)
-    int *lvl_off;    // [AMR_MAXLV+1] offsets into lvl_leaf
+    int *lvl_leaf;   // work order of the level-ordered kernels (see k_regrid_topo)
+    int *lvl_off;    // lvl_off[AMR_MAXLV] = number of entries of lvl_leaf
+    int *nbinfo;     // [k][NBI_STRIDE] neighbour record of lvl_leaf[k]
+    int *plan_c2, *plan_c1, *plan_hg;  // [k][PLAN_INTS][ring] fill plans of lvl_leaf[k]
     int *freelist;   // ring buffer of the first ids of freed quartets
     int *ref_list, *ref_c1, *der_list;
     Counters* cnt;

@@ -32,53 +32,62 @@ struct Geo {
     }
 };
 
-// RN(a/b) given yb = RN(1/b). q = RN(a*yb) is a faithful approximation of
-// a/b, the remainder r = a - q*b is exact in one FMA, and RN(q + r*yb) is the
-// correctly rounded quotient: Markstein's theorem (P. W. Markstein, "Computation
-// of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
-// Develop. 34(1), 1990; Muller et al., Handbook of Floating-Point Arithmetic,
-// ch. 4). The theorem needs normal operands and no underflow: quotients
-// outside [2^-960, 2^1000] (zero, tiny, huge, non-finite) take the plain
-// IEEE division. Checked bit for bit against IEEE division by
-// amrlbm_selftest_division.
-__device__ __forceinline__ double div_rn(double a, double b, double yb) {
-    const double q = a * yb;
-    // biased exponent of q in [63, 2023] <=> 2^-960 <= |q| < 2^1001
-    const unsigned e = ((unsigned)__double2hiint(q) >> 20) & 0x7ffu;
-    if (e - 63u <= 1960u) {
+// Exact FP64 division by b given yb = RN(1/b). q = RN(a*yb) is a faithful
+// approximation of a/b, the remainder r = a - q*b is exact in one FMA, and
+// RN(q + r*yb) is the correctly rounded quotient: Markstein's theorem
+// (P. W. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Develop. 34(1), 1990; Muller et al.,
+// Handbook of Floating-Point Arithmetic, ch. 4). The theorem needs a normal
+// quotient away from underflow and overflow. Div<false> evaluates the
+// formula without a branch, returns the exact signed zero for a zero
+// dividend, and ORs into `bad` whether any other quotient fell outside
+// [2^-960, 2^1001); a caller that sees `bad` recomputes with Div<true>, plain
+// IEEE division. Either way every quotient equals the IEEE one (checked bit
+// for bit by amrlbm_selftest_division).
+template <bool SAFE>
+struct Div {
+    unsigned bad = 0;
+    __device__ __forceinline__ double operator()(double a, double b, double yb) {
+        if (SAFE) return a / b;
+        const double q = a * yb;
         const double r = __fma_rn(-q, b, a);
-        return __fma_rn(r, yb, q);
+        const double q1 = __fma_rn(r, yb, q);
+        const unsigned ha = (unsigned)__double2hiint(a), la = (unsigned)__double2loint(a);
+        const bool a0 = ((ha & 0x7fffffffu) | la) == 0u;
+        const unsigned e = ((unsigned)__double2hiint(q) >> 20) & 0x7ffu;
+        bad |= (unsigned)((e - 63u > 1960u) & !a0);
+        return a0 ? q : q1;
     }
-    return a / b;
-}
-__device__ __forceinline__ double div3(double a) { return div_rn(a, 3.0, 1.0 / 3.0); }
-__device__ __forceinline__ double div6(double a) { return div_rn(a, 6.0, 1.0 / 6.0); }
-__device__ __forceinline__ double div12(double a) { return div_rn(a, 12.0, 1.0 / 12.0); }
-__device__ __forceinline__ double div36(double a) { return div_rn(a, 36.0, 1.0 / 36.0); }
+    __device__ __forceinline__ double d3(double a) { return (*this)(a, 3.0, 1.0 / 3.0); }
+    __device__ __forceinline__ double d6(double a) { return (*this)(a, 6.0, 1.0 / 6.0); }
+    __device__ __forceinline__ double d12(double a) { return (*this)(a, 12.0, 1.0 / 12.0); }
+    __device__ __forceinline__ double d36(double a) { return (*this)(a, 36.0, 1.0 / 36.0); }
+};
 
 // Gradient_ED_AMR (LBM_Subroutines.f90:281-289) from a directional
 // derivative functor E(k)
-template <class EF>
-__device__ __forceinline__ void gradient_ed_f(EF E, double& Dx, double& Dy) {
-    Dx = div3(E(2) - E(4)) + div12(E(6) - E(7) - E(8) + E(9));
-    Dy = div3(E(3) - E(5)) + div12(E(6) + E(7) - E(8) - E(9));
+template <class DV, class EF>
+__device__ __forceinline__ void gradient_ed_f(DV& dv, EF E, double& Dx, double& Dy) {
+    Dx = dv.d3(E(2) - E(4)) + dv.d12(E(6) - E(7) - E(8) + E(9));
+    Dy = dv.d3(E(3) - E(5)) + dv.d12(E(6) + E(7) - E(8) - E(9));
 }
 
 // Gradient_AMR (LBM_Subroutines.f90:293-312) at one cell; inv_dx = 1/dx (dx
 // is a power of two, so the product equals the quotient)
-template <class CF>
-__device__ __forceinline__ void gradient_iso_f(double inv_dx, CF Cs, double& DcDx, double& DcDy) {
-    DcDx = (div3(Cs(1, 0) - Cs(-1, 0)) + div12(Cs(1, 1) + Cs(1, -1) - Cs(-1, 1) - Cs(-1, -1))) *
+template <class DV, class CF>
+__device__ __forceinline__ void gradient_iso_f(DV& dv, double inv_dx, CF Cs, double& DcDx,
+                                               double& DcDy) {
+    DcDx = (dv.d3(Cs(1, 0) - Cs(-1, 0)) + dv.d12(Cs(1, 1) + Cs(1, -1) - Cs(-1, 1) - Cs(-1, -1))) *
            inv_dx;
-    DcDy = (div3(Cs(0, 1) - Cs(0, -1)) + div12(Cs(1, 1) + Cs(-1, 1) - Cs(1, -1) - Cs(-1, -1))) *
+    DcDy = (dv.d3(Cs(0, 1) - Cs(0, -1)) + dv.d12(Cs(1, 1) + Cs(-1, 1) - Cs(1, -1) - Cs(-1, -1))) *
            inv_dx;
 }
 
 // Laplacian_AMR + Chemical_Potential_AMR (LBM_Subroutines.f90:94-112,316-333)
-template <class CF>
-__device__ __forceinline__ double chem_pot_f(const PhysD& ph, double inv_dx2, CF Cs) {
-    const double D2C = div6(Cs(-1, -1) + Cs(1, -1) + Cs(-1, 1) + Cs(1, 1) +
-                            4.0 * (Cs(0, -1) + Cs(-1, 0) + Cs(1, 0) + Cs(0, 1)) - 20.0 * Cs(0, 0));
+template <class DV, class CF>
+__device__ __forceinline__ double chem_pot_f(DV& dv, const PhysD& ph, double inv_dx2, CF Cs) {
+    const double D2C = dv.d6(Cs(-1, -1) + Cs(1, -1) + Cs(-1, 1) + Cs(1, 1) +
+                             4.0 * (Cs(0, -1) + Cs(-1, 0) + Cs(1, 0) + Cs(0, 1)) - 20.0 * Cs(0, 0));
     const double c = Cs(0, 0);
     return ph.Beta4 * c * (c - 1.0) * (c - 0.5) - ph.kappa * D2C * inv_dx2;
 }

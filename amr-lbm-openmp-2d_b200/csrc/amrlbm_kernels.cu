@@ -423,43 +423,55 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_topo(DevState s, i
         }
     }
     __syncthreads();
-    // ---- Array_of_Leaf_Blocks + per-level lists + resolved neighbours
+    // ---- Array_of_Leaf_Blocks, resolved neighbours, level range
     const int nb = cnt->nblks;
     const int nleaf = compact(nb, s.leaf, 0, [&](int id) { return s.is_leaf[id] != 0; });
-    int off = 0;
-    int lo = 1 << 30, hi = -(1 << 30);
-    for (int L = 0; L < AMR_MAXLV; ++L) {
-        if (threadIdx.x == 0) s.lvl_off[L] = off;
-        const int c = compact(nb, s.lvl_leaf, off,
-                              [&](int id) { return s.is_leaf[id] != 0 && s.level[id] == L; });
-        if (c > 0) {
-            lo = min(lo, L);
-            hi = max(hi, L);
-        }
-        off += c;
-    }
+    __shared__ int s_lo, s_hi;
     if (threadIdx.x == 0) {
-        s.lvl_off[AMR_MAXLV] = off;
+        s_lo = 1 << 30;
+        s_hi = -(1 << 30);
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < nleaf; m += blockDim.x) {
+        const int n = s.leaf[m];
+        for (int k = 1; k <= 8; ++k) s.nbr[8 * n + k - 1] = resolve_chk(s, n, k);
+        s.ring_out[n] = 0;
+        atomicMin(&s_lo, s.level[n]);
+        atomicMax(&s_hi, s.level[n]);
+    }
+    __syncthreads();
+    // leaves whose ghost rings (C and h/g) a finer neighbour's coarse-to-fine
+    // fill reads: they publish their rings, their finer neighbours wait
+    for (int m = threadIdx.x; m < nleaf; m += blockDim.x) {
+        const int n = s.leaf[m];
+        for (int k = 0; k < 8; ++k) {
+            const int b = s.nbr[8 * n + k];
+            if (b > 0 && s.level[b] == s.level[n] - 1) s.ring_out[b] = 1;
+        }
+    }
+    __syncthreads();
+    const int lo = s_lo, hi = s_hi;
+    // work order of the level-ordered kernels: first the leaves others wait
+    // on (by level), then the rest (by level); a waited-on leaf always comes
+    // before its waiters
+    int off = 0;
+    for (int pass = 1; pass >= 0; --pass)
+        for (int L = lo; L <= hi; ++L)
+            off += compact(nleaf, s.lvl_leaf, off, [&](int m) {
+                const int n = s.leaf[m - 1];
+                return s.ring_out[n] == pass && s.level[n] == L;
+            });
+    // compact() stored positions 1..nleaf: turn them into block ids
+    __syncthreads();
+    for (int m = threadIdx.x; m < nleaf; m += blockDim.x) s.lvl_leaf[m] = s.leaf[s.lvl_leaf[m] - 1];
+    if (threadIdx.x == 0) {
+        s.lvl_off[AMR_MAXLV] = nleaf;
         cnt->nleaf = nleaf;
         cnt->leaf_min = lo;
         cnt->leaf_max = hi;
         if (set_levels) {
             cnt->level_min = lo;
             cnt->level_max = hi;
-        }
-    }
-    for (int m = threadIdx.x; m < nleaf; m += blockDim.x) {
-        const int n = s.leaf[m];
-        for (int k = 1; k <= 8; ++k) s.nbr[8 * n + k - 1] = resolve_chk(s, n, k);
-        s.ring_out[n] = 0;
-    }
-    __syncthreads();
-    // leaves whose h/g ghost ring a finer neighbour's coarse-to-fine fill reads
-    for (int m = threadIdx.x; m < nleaf; m += blockDim.x) {
-        const int n = s.leaf[m];
-        for (int k = 0; k < 8; ++k) {
-            const int b = s.nbr[8 * n + k];
-            if (b > 0 && s.level[b] == s.level[n] - 1) s.ring_out[b] = 1;
         }
     }
 }

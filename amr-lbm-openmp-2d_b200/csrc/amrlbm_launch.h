@@ -21,8 +21,7 @@ struct LaunchCfg {
 
 void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width,
                    int consumer);
-// write_all: every ring goes to memory (else only rings a finer neighbour reads)
-void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int write_all);
+void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_collide(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_macro_h(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_macro_g(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
@@ -37,6 +36,9 @@ void launch_restrict(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 // leaves (what the next Determine_Min_Max_Levels returns).
 void launch_regrid_topo(const DevState& s, cudaStream_t st, int mode, int lmin, int lmax,
                         int set_levels);
+// neighbour records and ghost-cell fill plans of the leaves in work order;
+// after every change of the topology
+void launch_build_plans(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_prolong(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_zero_children(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_flag_level(const DevState& s, cudaStream_t st, int level);
