@@ -3,6 +3,7 @@
 // driver's start-up, CUDA-graph stepping, diagnostics and timing.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1083,3 +1084,153 @@ int upload_blocks(amrlbm_ctx* ctx, int n, const int* ids, const double* h, const
     return 0;
 }
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Field download without allocation.
+//
+// amrlbm_download_fields stages through buffers it grows on demand: device
+// memory for the block ids and the staged records (cudaMalloc) and
+// page-locked host memory (cudaMallocHost). Some callers cannot have that:
+// a host code that sizes all of its device memory once at start-up, as a
+// Fortran driver sharing a GPU with other jobs under a fixed memory budget
+// does, and an output hook that runs between time steps, where a call into
+// the allocator may synchronise the device and would stall the stepping
+// stream. The variant below stages through one fixed scratch area per
+// device, a file-scope __device__ array, and copies each field straight into
+// the caller's array.
+//
+// Limits: at most AMRLBM_NOALLOC_STAGE_DOUBLES doubles of requested field
+// data and AMRLBM_NOALLOC_MAX_BLOCKS blocks per call; larger requests are
+// rejected with AMRLBM_ERR_CAPACITY before anything runs. Nothing in the
+// scratch has to start at zero: every element the call reads back was
+// written earlier in the same call. The scratch is shared by every context
+// on the device, so calls that overlap in time on one device (from two host
+// threads, or on two contexts' streams) race on it; the caller serialises
+// them.
+namespace {
+
+static __device__ __align__(256) double g_noalloc_stage[AMRLBM_NOALLOC_STAGE_DOUBLES];
+static __device__ __align__(256) int g_noalloc_ids[AMRLBM_NOALLOC_MAX_BLOCKS];
+
+constexpr int kNoallocDevices = 64;
+struct NoallocScratch {
+    std::atomic<double*> stage{nullptr};
+    std::atomic<int*> ids{nullptr};
+};
+NoallocScratch g_noalloc_scratch[kNoallocDevices];
+
+// Set-up, once per device, with that device current: the device addresses of
+// the scratch arrays (cudaGetSymbolAddress allocates nothing). The first call
+// on a device does this; a caller that records its work into a stream
+// capture makes that first call before the capture starts.
+cudaError_t noalloc_scratch(int dev, double** stage, int** ids) {
+    if (dev < 0 || dev >= kNoallocDevices) return cudaErrorInvalidDevice;
+    NoallocScratch& sc = g_noalloc_scratch[dev];
+    double* st = sc.stage.load();
+    int* id = sc.ids.load();
+    if (!st || !id) {
+        cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&st), g_noalloc_stage);
+        if (e != cudaSuccess) return e;
+        e = cudaGetSymbolAddress(reinterpret_cast<void**>(&id), g_noalloc_ids);
+        if (e != cudaSuccess) return e;
+        sc.stage.store(st);
+        sc.ids.store(id);
+    }
+    *stage = st;
+    *ids = id;
+    return cudaSuccess;
+}
+
+// k_transfer's pool -> staging direction with the staging laid out field by
+// field: field f of block i at stage[off[f] + i*size(f)], in the same
+// per-block layout (off[f] < 0: field not requested)
+__global__ void k_download_fieldwise(DevState s, const int* ids, int n, double* stage,
+                                     long long off0, long long off1, long long off2, long long off3,
+                                     long long off4, long long off5) {
+    const int nx = s.nx, ny = s.ny;
+    const int hs = 9 * (nx + 2) * (ny + 2), cs = (nx + 4) * (ny + 4), ps = nx * ny;
+    const long long off[6] = {off0, off1, off2, off3, off4, off5};
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int b = ids[i];
+        for (int f = 0; f < 2; ++f) {
+            if (off[f] < 0) continue;
+            const double* A = f ? s.Ag : s.Ah;
+            const double* B = f ? s.Bg : s.Bh;
+            double* r = stage + off[f] + (size_t)i * hs;
+            for (int e = threadIdx.x; e < hs; e += blockDim.x) {
+                const int q = e % 9 + 1, xy = e / 9, x = xy % (nx + 2), y = xy / (nx + 2);
+                const bool in = x >= 1 && x <= nx && y >= 1 && y <= ny;
+                r[e] = in ? B[b_idx(s, b, q, x, y)] : A[a_idx(s, b, q, x, y)];
+            }
+        }
+        if (off[2] >= 0) {
+            double* r = stage + off[2] + (size_t)i * cs;
+            for (int e = threadIdx.x; e < cs; e += blockDim.x)
+                r[e] = s.C[c_idx(s, b, e % (nx + 4) - 1, e / (nx + 4) - 1)];
+        }
+        for (int f = 0; f < 3; ++f) {
+            if (off[3 + f] < 0) continue;
+            const double* A = f == 0 ? s.P : (f == 1 ? s.Ux : s.Uy);
+            double* r = stage + off[3 + f] + (size_t)i * ps;
+            for (int e = threadIdx.x; e < ps; e += blockDim.x) r[e] = A[(size_t)b * s.pplane + e];
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int amrlbm_download_fields_noalloc(amrlbm_ctx* ctx, int32_t n, const int32_t* ids,
+                                              double* h, double* g, double* C, double* P,
+                                              double* Ux, double* Uy) {
+    if (!ctx || n < 0 || (n > 0 && !ids)) return AMRLBM_ERR_ARG;
+    if (n == 0) return AMRLBM_OK;
+    for (int i = 0; i < n; ++i)
+        if (ids[i] < 1 || ids[i] > ctx->prm.max_blks) return AMRLBM_ERR_ARG;
+    const int nx = ctx->prm.nx, ny = ctx->prm.ny;
+    const size_t hs = (size_t)9 * (nx + 2) * (ny + 2), cs = (size_t)(nx + 4) * (ny + 4),
+                 ps = (size_t)nx * ny;
+    double* dst[6] = {h, g, C, P, Ux, Uy};
+    const size_t sz[6] = {hs, hs, cs, ps, ps, ps};
+    long long off[6];
+    size_t used = 0;
+    for (int f = 0; f < 6; ++f) {
+        off[f] = dst[f] ? (long long)used : -1;
+        if (dst[f]) used += (size_t)n * sz[f];
+    }
+    if (n > AMRLBM_NOALLOC_MAX_BLOCKS || used > (size_t)AMRLBM_NOALLOC_STAGE_DOUBLES)
+        return AMRLBM_ERR_CAPACITY;
+    if (used == 0) return AMRLBM_OK;
+    // the device that holds the context's pool, current for this call
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, ctx->s.C) != cudaSuccess) return AMRLBM_ERR_CUDA;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return AMRLBM_ERR_CUDA;
+    if (prev != pa.device && cudaSetDevice(pa.device) != cudaSuccess) return AMRLBM_ERR_CUDA;
+    int rc = AMRLBM_OK;
+    double* stage = nullptr;
+    int* dids = nullptr;
+    cudaError_t e = noalloc_scratch(pa.device, &stage, &dids);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dids, ids, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, ctx->st);
+    if (e == cudaSuccess) {
+        k_download_fieldwise<<<ctx->lc.grid_leaves, 256, 0, ctx->st>>>(
+            ctx->s, dids, n, stage, off[0], off[1], off[2], off[3], off[4], off[5]);
+        count_launches(1);
+        e = cudaGetLastError();
+    }
+    for (int f = 0; f < 6 && e == cudaSuccess; ++f)
+        if (dst[f])
+            e = cudaMemcpyAsync(dst[f], stage + off[f], (size_t)n * sz[f] * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    if (e != cudaSuccess) rc = AMRLBM_ERR_CUDA;
+    if (rc == AMRLBM_OK) {  // a pending device-side error status, as the other calls report it
+        int st[2] = {0, 0};
+        if (cudaMemcpy(st, &ctx->s.cnt->error, sizeof(st), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = AMRLBM_ERR_CUDA;
+        else if (st[0] != 0)
+            rc = st[0];
+    }
+    if (prev != pa.device) cudaSetDevice(prev);
+    return rc;
+}

@@ -51,7 +51,8 @@ enum {
     AMRLBM_ERR_NAN = 5,        /* non-finite field value found by diagnostics  */
     AMRLBM_ERR_DANGLING = 6,   /* neighbour pointer into a freed block's child array */
     AMRLBM_ERR_STATE = 7,      /* call out of order (e.g. step before init)    */
-    AMRLBM_ERR_TIMEOUT = 8     /* a bounded device wait ran out                */
+    AMRLBM_ERR_TIMEOUT = 8,    /* a bounded device wait ran out                */
+    AMRLBM_ERR_CAPACITY = 9    /* request larger than a fixed scratch area      */
 };
 
 /* flag bits of amrlbm_get_topology / amrlbm_set_topology */
@@ -221,6 +222,25 @@ int64_t amrlbm_launch_count(const amrlbm_ctx* ctx);
 int amrlbm_selftest_division(uint64_t n, uint64_t seed, double divisor, uint64_t* mismatches);
 /* Writes a buffer larger than the L2 cache on the context's stream. */
 int amrlbm_flush_l2(amrlbm_ctx* ctx);
+
+/* ---- download without allocation ----------------------------------------
+ * No counterpart in the reference, whose fields live in host memory.
+ * amrlbm_download_fields with the same arguments and results, for callers
+ * that must not allocate once set up (a host code with a fixed device-memory
+ * budget, an output hook between time steps): it stages through a fixed
+ * scratch area per device instead of buffers it allocates, and copies every
+ * field straight into the caller's array. At most AMRLBM_NOALLOC_MAX_BLOCKS
+ * blocks and AMRLBM_NOALLOC_STAGE_DOUBLES doubles of requested fields (n times
+ * the sizes of the non-NULL fields) per call, else AMRLBM_ERR_CAPACITY and
+ * nothing runs; split larger downloads into several calls. The scratch is
+ * shared by all contexts on a device: calls that overlap in time on one
+ * device race on it and must be serialised by the caller. The first call on
+ * a device sets the scratch up (no allocation); it returns no message
+ * through amrlbm_last_error. */
+#define AMRLBM_NOALLOC_STAGE_DOUBLES 524288 /* 4 MiB */
+#define AMRLBM_NOALLOC_MAX_BLOCKS 16384
+int amrlbm_download_fields_noalloc(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, double* h,
+                                   double* g, double* C, double* P, double* Ux, double* Uy);
 
 #ifdef __cplusplus
 }
