@@ -86,9 +86,16 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+PROFILE_FILES = {
+    "fill_c2_collide": "k_fill_c_collide__rising_bubble_256x512_L3.md",
+    "fill_hg_stream_macro_h": "k_fill_hg_stream__rising_bubble_256x512_L3.md",
+}
+
+
 def profile_traffic(kernel_name):
-    """dram bytes per launch from a committed ncu summary, if one exists."""
-    path = os.path.join(ROOT, "profiles", f"{kernel_name}.md")
+    """dram bytes per launch from the committed ncu summary of the kernel on
+    this workload, if one exists."""
+    path = os.path.join(ROOT, "profiles", PROFILE_FILES.get(kernel_name, kernel_name + ".md"))
     try:
         with open(path) as f:
             for line in f:

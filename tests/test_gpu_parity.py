@@ -194,3 +194,24 @@ def test_large_workload_topology_and_fields():
         compare_counts(gpu, orc)
         compare_topology(gpu, orc)
         compare_fields(gpu, orc)
+
+
+@pytest.mark.parametrize("name", ["reference_default", "small_16x16"])
+def test_device_matches_golden_fixtures(name):
+    """The device path against the committed fixtures of tests/golden/
+    (start-up state and the state after a few time steps, bit for bit)."""
+    import json
+    import os
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    from make_golden import CASES, snapshot
+    with open(os.path.join(here, "golden", f"oracle_{name}.json")) as f:
+        want = json.load(f)
+    factory, steps = CASES[name]
+    p = factory()
+    with AmrLbm(p) as gpu:
+        gpu.initialize_rising_bubble()
+        assert snapshot(gpu, p) == want["init"]
+        gpu.main_loop(steps)
+        assert snapshot(gpu, p) == want["after_steps"]
