@@ -395,10 +395,13 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
         return AMRLBM_ERR_ARG;
     if ((p->dx0 >> p->max_levels) < 1) return AMRLBM_ERR_ARG;  // dx stays an integer >= 1
     if (p->dx0 & (p->dx0 - 1)) return AMRLBM_ERR_ARG;  // powers of two (L0/nx = 2**maxLevels)
-    {  // fill plans hold 32-bit offsets into the A pool
+    {  // fill plans hold 31-bit offsets into the A pool and 31-bit plan indices
         const size_t ap = ((size_t)p->nx + 5 + 3) / 4 * 4;
         const size_t aplane = ((p->ny + 2) * ap + 15) / 16 * 16;
-        if (((size_t)p->max_blks + 1) * 9 * aplane >= (1ull << 32)) return AMRLBM_ERR_ARG;
+        const size_t r2 = 4 * ((size_t)p->nx + p->ny) + 16;
+        if (((size_t)p->max_blks + 1) * 9 * aplane >= (1ull << 31) ||
+            ((size_t)p->max_blks + 1) * r2 >= (1ull << 31))
+            return AMRLBM_ERR_ARG;
     }
     int dev = 0, cc = 0, sms = 0;
     if (p->device >= 0 && cudaSetDevice(p->device) != cudaSuccess) return AMRLBM_ERR_CUDA;
@@ -470,6 +473,10 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     AL(plan_c2, int, NB * PLAN_INTS * (size_t)(4 * (nx + ny) + 16));
     AL(plan_c1, int, NB * PLAN_INTS * (size_t)(2 * (nx + ny) + 4));
     AL(plan_hg, int, NB * PLAN_INTS * (size_t)(2 * (nx + ny) + 4));
+    AL(fillinfo, int, 3 * NQUEUES);
+    AL(interp_c2, int, 2 * NB * (size_t)(4 * (nx + ny) + 16));
+    AL(interp_c1, int, 2 * NB * (size_t)(2 * (nx + ny) + 4));
+    AL(interp_hg, int, 2 * NB * (size_t)(2 * (nx + ny) + 4));
     AL(freelist, int, (size_t)s.fl_cap);
     AL(ref_list, int, NB);
     AL(ref_c1, int, NB);

@@ -45,7 +45,7 @@ enum { Q_FILLC = 0, Q_FILLHG = 1, Q_FILLC1 = 2, NQUEUES = 3 };
 // per-leaf records of the level-ordered kernels, indexed by work-order
 // position: neighbour record (NBI_STRIDE ints) and one fill plan per ghost
 // cell (PLAN_INTS ints: kind/weights word + 9 source offsets)
-enum { NBI_STRIDE = 40, PLAN_INTS = 10 };
+enum { NBI_STRIDE = 48, PLAN_INTS = 10 };
 
 // ---------------------------------------------------------------------------
 // The block pool. Block ids are 1..max_blks (slot 0 unused).
@@ -78,6 +78,13 @@ struct DevState {
     int *lvl_off;    // lvl_off[AMR_MAXLV] = number of entries of lvl_leaf
     int *nbinfo;     // [k][NBI_STRIDE] neighbour record of lvl_leaf[k]
     int *plan_c2, *plan_c1, *plan_hg;  // [k][PLAN_INTS][ring] fill plans of lvl_leaf[k]
+    // [q]: a fill of queue q needs level order; [NQUEUES+q], [2*NQUEUES+q]:
+    // copied and fine-to-coarse ghost cells of that fill
+    int* fillinfo;
+    // units of the flat fills, 2 ints each in 2*(max_blks+1)*R ints: copies
+    // (dest, source offset) from the front, fine-to-coarse cells (dest,
+    // k*R + t) from the back
+    int *interp_c2, *interp_c1, *interp_hg;
     int *freelist;   // ring buffer of the first ids of freed quartets
     int *ref_list, *ref_c1, *der_list;
     Counters* cnt;

@@ -3,16 +3,20 @@
 // every operation the reference writes is rounded on its own and in its
 // order; exact FMAs appear only inside the division of amrlbm_fast.cuh.
 //
-// Level-ordered launches. The reference fills ghost cells level by level
-// (Fill_Ghost_Cells_C.f90:8-38): a coarse-to-fine fill reads the coarse
-// neighbour's ghost ring, written one level earlier. One launch serves all
-// levels here: CTAs claim leaves from a queue in which every leaf that a
-// finer neighbour reads precedes its readers (k_regrid_topo); a leaf whose
-// fill reads a coarser neighbour's ring waits (bounded spin) until that
-// neighbour has published it (a per-block flag). The waited-on leaf was
-// claimed earlier by a CTA that is running, so the wait always ends. After its fill a CTA goes on with the
-// work that needs only its own ring (collision, streaming, macroscopic
-// values): one launch does "fill + consumer", no grid-wide barrier.
+// Ghost fills without grid-wide level loops. The reference fills ghost cells
+// level by level (Fill_Ghost_Cells_C.f90:8-38): a coarse-to-fine fill reads
+// the coarse neighbour's ghost ring, written one level earlier. Here, after
+// every topology change, each ghost cell of each leaf gets a fill plan (copy,
+// fine-to-coarse or coarse-to-fine interpolation, with its source offsets).
+// When every coarse-to-fine source is an interior cell or a coarser
+// neighbour's ghost cell that is itself a copy or a fine-to-coarse value (the
+// usual case), two flat launches fill all rings: copies and fine-to-coarse
+// cells first, coarse-to-fine cells second; the consumer launch (collision,
+// streaming or macroscopic values) applies the walls. Otherwise the consumer
+// launch fills level by level first: CTAs claim leaves from a queue in which
+// every leaf a finer neighbour reads precedes its readers, a leaf waits
+// (bounded spin) for its coarser neighbours' flags, and no grid barrier is
+// needed.
 #include <cstdio>
 
 #include "amrlbm_fast.cuh"
@@ -42,12 +46,15 @@ __device__ __forceinline__ int ghost_dir(int x, int y, int nx, int ny) {
 }
 
 // per-direction neighbour data of the block being filled, loaded once into
-// shared memory: resolved id, its level, leaf flag and first child
+// shared memory: resolved id, its level, leaf flag and first child (index 0:
+// the block itself); wait: the directions of coarser neighbours, whose rings
+// a level-ordered fill waits for
 struct NbInfo {
     int id[9], lev[9], leaf[9], c1[9];
     int bi, bj;
+    int wait;
 };
-constexpr int NBI_INTS = (int)(sizeof(NbInfo) / sizeof(int));  // 38
+constexpr int NBI_INTS = (int)(sizeof(NbInfo) / sizeof(int));
 static_assert(NBI_INTS <= NBI_STRIDE, "NbInfo record");
 
 // ---------------------------------------------------------------------------
@@ -211,69 +218,107 @@ __device__ __forceinline__ void ring2_xy(int t, int nx, int ny, int& x, int& y) 
 __host__ __device__ __forceinline__ int ring2_len(int nx, int ny) { return 4 * (nx + ny) + 16; }
 __host__ __device__ __forceinline__ int ring1_len(int nx, int ny) { return 2 * (nx + ny) + 4; }
 
+
 // ---------------------------------------------------------------------------
 // Neighbour records and fill plans of every leaf, in work order (one CTA per
 // leaf). The neighbour data is what Fill_Ghost_Cells_* reads through the
 // block pointers (Fill_Ghost_Cells_C.f90:8-38): resolved neighbour ids, their
-// levels, leaf flags and first children, plus the block's own id, level,
-// ring_out flag and the mask of directions whose neighbour is one level
-// coarser (the fills that wait for that neighbour's ring).
+// levels, leaf flags and first children, plus the block's own id, level and
+// ring_out flag.
+//
+// Coarse-to-fine cells read the coarser neighbour's ring, which the
+// reference fills one level earlier. Where such a ring cell is itself a copy
+// or a fine-to-coarse interpolation of interiors, the plan refers to that
+// cell's own plan entry and the fill evaluates it in place, with the same
+// operations the neighbour's fill uses, so the fill need not wait. Only where
+// it is a coarse-to-fine or wall cell does the record's wait mask make the
+// fill wait for the neighbour's flag.
+__device__ void load_nbinfo(const DevState& s, int n, NbInfo& r) {
+    for (int j = 0; j < 8; ++j) {
+        const int b = s.nbr[8 * n + j];
+        r.id[j + 1] = b;
+        r.lev[j + 1] = (b > 0) ? s.level[b] : -1;
+        r.leaf[j + 1] = (b > 0) ? (int)s.is_leaf[b] : 0;
+        r.c1[j + 1] = (b > 0) ? s.child[4 * b] : 0;
+    }
+    r.id[0] = n;
+    r.lev[0] = s.level[n];
+    r.leaf[0] = (int)s.ring_out[n];
+    r.c1[0] = 0;
+    r.bi = s.bi[n];
+    r.bj = s.bj[n];
+    r.wait = 0;
+}
+
 template <int N>
 __global__ void k_build_plans(DevState s) {
     const Geo<N> G(s);
     __shared__ NbInfo nbi;
+    __shared__ NbInfo cnb[9];  // coarser neighbours' records
     const int nx = G.nx, ny = G.ny, R2 = ring2_len(nx, ny), R1 = ring1_len(nx, ny);
     const int total = s.lvl_off[AMR_MAXLV];
     const int t = threadIdx.x;
     for (int k = blockIdx.x; k < total; k += gridDim.x) {
         const int n = s.lvl_leaf[k];
-        if (t < 8) {
-            const int b = s.nbr[8 * n + t];
-            nbi.id[t + 1] = b;
-            nbi.lev[t + 1] = (b > 0) ? s.level[b] : -1;
-            nbi.leaf[t + 1] = (b > 0) ? (int)s.is_leaf[b] : 0;
-            nbi.c1[t + 1] = (b > 0) ? s.child[4 * b] : 0;
-        } else if (t == 8) {
-            nbi.bi = s.bi[n];
-            nbi.bj = s.bj[n];
-        } else if (t == 9) {
-            nbi.id[0] = n;
-            nbi.lev[0] = s.level[n];
-            nbi.leaf[0] = (int)s.ring_out[n];
+        if (t == 0) load_nbinfo(s, n, nbi);
+        __syncthreads();
+        const int L = nbi.lev[0];
+        if (t >= 1 && t <= 8 && nbi.id[t] > 0 && nbi.lev[t] == L - 1) {
+            load_nbinfo(s, nbi.id[t], cnb[t]);
+            atomicOr(&nbi.wait, 1 << t);
         }
         __syncthreads();
-        if (t == 0) {
-            int m = 0;
-            for (int d = 1; d <= 8; ++d)
-                if (nbi.id[d] > 0 && nbi.lev[d] == nbi.lev[0] - 1) m |= 1 << d;
-            nbi.c1[0] = m;
-        }
+        // one plan type: queue q, plan array, unit lists of the flat fill
+        // (copies (dest, source) from the front, fine-to-coarse cells (dest,
+        // k*R + t) from the back, 2 ints each), ring length R, ring-2
+        // indexing, offsets into the A pool (else C)
+        auto build = [&](int q, int* plans, int* units, int R, bool two, bool afield) {
+            auto off = [&](int blk, int xx, int yy) -> long long {
+                return afield ? (long long)G.a(blk, 1, xx, yy) : (long long)G.c(blk, xx, yy);
+            };
+            const size_t cap2 = 2 * (size_t)(s.max_blks + 1) * R;
+            for (int i = t; i < R; i += blockDim.x) {
+                int x, y;
+                if (two)
+                    ring2_xy(i, nx, ny, x, y);
+                else
+                    ring1_xy(i, nx, ny, x, y);
+                const int d = ghost_dir(x, y, nx, ny);
+                bool deep = false;
+                GPlan P;
+                ghost_plan(nbi, nx, ny, L, d, x, y,
+                           [&](int blk, int xx, int yy) -> long long {
+                               // a coarser neighbour's ghost cell must be a copy or
+                               // a fine-to-coarse value (its neighbour on that
+                               // side exists and has its level) for the flat fill
+                               const bool ring = xx < 1 || xx > nx || yy < 1 || yy > ny;
+                               if (ring && blk == nbi.id[d] && nbi.lev[d] == L - 1) {
+                                   const int dd = ghost_dir(xx, yy, nx, ny);
+                                   if (!nbi.leaf[d] || cnb[d].id[dd] <= 0 || cnb[d].lev[dd] != L - 1)
+                                       deep = true;
+                               }
+                               return off(blk, xx, yy);
+                           },
+                           P);
+                plan_store(plans + (size_t)k * R * PLAN_INTS, R, i, P);
+                if (deep || P.kind < 0) atomicOr(&s.fillinfo[q], 1);  // a level jump is reported there
+                if (P.kind == 1) {
+                    const size_t j = atomicAdd(&s.fillinfo[NQUEUES + q], 1);
+                    units[2 * j] = (int)off(n, x, y);
+                    units[2 * j + 1] = (int)(unsigned)P.src[0];
+                } else if (P.kind == 2) {
+                    const size_t j = atomicAdd(&s.fillinfo[2 * NQUEUES + q], 1);
+                    units[cap2 - 2 - 2 * j] = (int)off(n, x, y);
+                    units[cap2 - 1 - 2 * j] = k * R + i;
+                }
+            }
+        };
+        build(Q_FILLC, s.plan_c2, s.interp_c2, R2, true, false);
+        build(Q_FILLC1, s.plan_c1, s.interp_c1, R1, false, false);
+        build(Q_FILLHG, s.plan_hg, s.interp_hg, R1, false, true);
         __syncthreads();
         if (t < NBI_STRIDE)
             s.nbinfo[(size_t)k * NBI_STRIDE + t] = (t < NBI_INTS) ? reinterpret_cast<int*>(&nbi)[t] : 0;
-        const int L = nbi.lev[0];
-        auto offc = [&](int blk, int xx, int yy) { return (long long)G.c(blk, xx, yy); };
-        auto offa = [&](int blk, int xx, int yy) { return (long long)G.a(blk, 1, xx, yy); };
-        int* p2 = s.plan_c2 + (size_t)k * R2 * PLAN_INTS;
-        for (int i = t; i < R2; i += blockDim.x) {
-            int x, y;
-            ring2_xy(i, nx, ny, x, y);
-            GPlan P;
-            ghost_plan(nbi, nx, ny, L, ghost_dir(x, y, nx, ny), x, y, offc, P);
-            plan_store(p2, R2, i, P);
-        }
-        int* p1 = s.plan_c1 + (size_t)k * R1 * PLAN_INTS;
-        int* ph = s.plan_hg + (size_t)k * R1 * PLAN_INTS;
-        for (int i = t; i < R1; i += blockDim.x) {
-            int x, y;
-            ring1_xy(i, nx, ny, x, y);
-            const int d = ghost_dir(x, y, nx, ny);
-            GPlan P;
-            ghost_plan(nbi, nx, ny, L, d, x, y, offc, P);
-            plan_store(p1, R1, i, P);
-            ghost_plan(nbi, nx, ny, L, d, x, y, offa, P);
-            plan_store(ph, R1, i, P);
-        }
         __syncthreads();
     }
 }
@@ -313,7 +358,7 @@ __device__ __forceinline__ bool spin_flag(const int* flag) {
 // block-uniform, ends with a barrier
 __device__ __forceinline__ void wait_coarse(const DevState& s, int q, const NbInfo& nbi) {
     const int t = threadIdx.x;
-    if (t < 8 && ((nbi.c1[0] >> (t + 1)) & 1))
+    if (t < 8 && ((nbi.wait >> (t + 1)) & 1))
         if (!spin_flag(fill_flags(s, q) + nbi.id[t + 1])) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, q);
     __syncthreads();
 }
@@ -370,21 +415,43 @@ __device__ __forceinline__ void fill_phase(const DevState& s, int q, NbInfo* nbi
     }
 }
 
-// ---------------------------------------------------------------------------
-// C ghost ring of width w of the item at work position k (block n) from its
-// plans, into memory. pass 0: every cell that reads no coarser neighbour's
-// ring; pass 1: the coarse-to-fine cells. Kind 1 and 2 sources are
-// interiors nothing writes during the launch; kind 3 sources include a ring
-// written in it.
+// The same walls for a block whose ring is in memory (written by an earlier
+// launch) and, if T is given, in its shared C tile (index G.c(0,x,y)), which
+// then is the source. No barrier inside: the rows read and written differ.
 template <int N>
-__device__ void fill_c_ring(const DevState& s, const Geo<N>& G, int k, int n, int w, int pass) {
+__device__ void wall_c_rows(const DevState& s, const Geo<N>& G, int n, int w, bool w3, bool w4,
+                            double* T) {
+    const int nx = G.nx, ny = G.ny;
+    for (int idx = threadIdx.x; idx < (nx + 2 * w) * w * 2; idx += blockDim.x) {
+        const int X = idx % (nx + 2 * w) + 1 - w, a = (idx / (nx + 2 * w)) % w + 1;
+        const bool top = idx >= (nx + 2 * w) * w;
+        if (top ? !w4 : !w3) continue;
+        const int ys = top ? ny + 1 - a : a, yd = top ? ny + a : 1 - a;
+        const double v = T ? T[G.c(0, X, ys)] : ldcg(s.C + G.c(n, X, ys));
+        if (T) T[G.c(0, X, yd)] = v;
+        s.C[G.c(n, X, yd)] = v;
+    }
+}
+
+// which plan kinds a fill pass evaluates: 0 all, 1 all but coarse-to-fine
+// (before a wait), 2 coarse-to-fine only (after it)
+__device__ __forceinline__ bool pass_takes(int mode, int kind) {
+    return mode == 0 || ((kind == 3) == (mode == 2));
+}
+
+// C ghost ring of width w of the item at work position k (block n) from its
+// plans, into memory (level-ordered path). Kind 1 and 2 sources are
+// interiors nothing writes during the launch; kind 3 sources include a
+// coarser neighbour's ring written in it (read through L2 after the wait).
+template <int N>
+__device__ void fill_c_ring(const DevState& s, const Geo<N>& G, int k, int n, int w, int mode) {
     const int nx = G.nx, ny = G.ny;
     const int R = (w == 2) ? ring2_len(nx, ny) : ring1_len(nx, ny);
     const int* pl = ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)k * R * PLAN_INTS;
     for (int t = threadIdx.x; t < R; t += blockDim.x) {
         const int meta = __ldg(pl + t);
         const int kind = plan_kind(meta);
-        if (kind == 0 || ((kind == 3) != (pass == 1))) continue;
+        if (kind == 0 || !pass_takes(mode, kind)) continue;
         int x, y;
         if (w == 2)
             ring2_xy(t, nx, ny, x, y);
@@ -399,10 +466,12 @@ __device__ void fill_c_ring(const DevState& s, const Geo<N>& G, int k, int n, in
             v = __ldg(s.C + (unsigned)__ldg(pl + R + t));
         } else {
             double g[9];
+            if (kind == 2) {
 #pragma unroll
-            for (int i = 0; i < 9; ++i) {
-                const double* src = s.C + (unsigned)__ldg(pl + (1 + i) * R + t);
-                g[i] = (kind == 3) ? ldcg(src) : __ldg(src);
+                for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)__ldg(pl + (1 + i) * R + t));
+            } else {
+#pragma unroll
+                for (int i = 0; i < 9; ++i) g[i] = ldcg(s.C + (unsigned)__ldg(pl + (1 + i) * R + t));
             }
             v = plan_combine(meta, g);
         }
@@ -632,6 +701,117 @@ __device__ __forceinline__ void err_reduce(const DevState& s, int n, double mx, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Whether fill Q takes the flat path: no coarse-to-fine cell reads a coarser
+// neighbour's ghost cell that is itself coarse-to-fine or a wall cell, and
+// every leaf's level is in [LevelMin, LevelMax]. Else the consumer launch
+// fills level by level.
+__device__ __forceinline__ bool flat_fill(const DevState& s, int q) {
+    return s.fillinfo[q] == 0 && s.cnt->level_min <= s.cnt->leaf_min &&
+           s.cnt->level_max >= s.cnt->leaf_max;
+}
+
+// The copies and fine-to-coarse ghost cells of every leaf, one flat launch:
+// one thread per copied cell (and field: its 9 populations together), one per
+// fine-to-coarse cell (and field and population). Every source is an
+// interior cell no launch of this fill writes. The coarse-to-fine cells (which
+// read the copies and fine-to-coarse cells of coarser neighbours) and the
+// walls are left to the consumer launch.
+template <int N, int Q>
+__global__ void __launch_bounds__(256) k_fill_flat(DevState s) {
+    if (!flat_fill(s, Q)) return;
+    const Geo<N> G(s);
+    constexpr bool HG = (Q == Q_FILLHG);
+    constexpr int F = HG ? 2 : 1;
+    const int R = (Q == Q_FILLC) ? ring2_len(G.nx, G.ny) : ring1_len(G.nx, G.ny);
+    const int* plans = (Q == Q_FILLC) ? s.plan_c2 : (Q == Q_FILLC1 ? s.plan_c1 : s.plan_hg);
+    const int* units = (Q == Q_FILLC) ? s.interp_c2 : (Q == Q_FILLC1 ? s.interp_c1 : s.interp_hg);
+    const size_t cap2 = 2 * (size_t)(s.max_blks + 1) * R;
+    const int nc = s.fillinfo[NQUEUES + Q], ni = s.fillinfo[2 * NQUEUES + Q];
+    const int nA = nc * F, nB = ni * (HG ? 18 : 1);
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nA + nB; u += gridDim.x * blockDim.x) {
+        if (u < nA) {
+            const int j = u % nc, f = u / nc;
+            const unsigned dst = (unsigned)__ldg(units + 2 * j), src = (unsigned)__ldg(units + 2 * j + 1);
+            double* A = HG ? (f ? s.Ag : s.Ah) : s.C;
+            if (HG) {
+                double v[9];
+#pragma unroll
+                for (int i = 0; i < 9; ++i) v[i] = __ldg(A + src + (size_t)i * G.aplane);
+#pragma unroll
+                for (int i = 0; i < 9; ++i) A[dst + (size_t)i * G.aplane] = v[i];
+            } else {
+                A[dst] = __ldg(A + src);
+            }
+            continue;
+        }
+        const int v = u - nA, j = HG ? v / 18 : v, fq = HG ? v % 18 : 0;
+        const unsigned dst = (unsigned)__ldg(units + cap2 - 2 - 2 * (size_t)j);
+        const int e = __ldg(units + cap2 - 1 - 2 * (size_t)j);
+        const int* pl = plans + (size_t)(e / R) * R * PLAN_INTS + e % R;
+        const int meta = __ldg(pl);
+        double* A = HG ? (fq >= 9 ? s.Ag : s.Ah) : s.C;
+        const size_t qo = (size_t)(fq % 9) * (HG ? G.aplane : 0);
+        double g[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) g[i] = __ldg(A + (unsigned)__ldg(pl + (1 + i) * R) + qo);
+        A[dst + qo] = plan_combine(meta, g);
+    }
+}
+
+// The coarse-to-fine ghost cells of block n (work position c) on the flat
+// path, into its staged copy and into memory. Sources: the coarser
+// neighbour's interior and its copies / fine-to-coarse cells, written by
+// k_fill_flat. T: shared C tile (index G.c(0,x,y)).
+template <int N>
+__device__ void c2f_cells_c(const DevState& s, const Geo<N>& G, int c, int n, int w, double* T) {
+    const int nx = G.nx, ny = G.ny;
+    const int R = (w == 2) ? ring2_len(nx, ny) : ring1_len(nx, ny);
+    const int* pl = ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)c * R * PLAN_INTS;
+    for (int t = threadIdx.x; t < R; t += blockDim.x) {
+        const int meta = __ldg(pl + t);
+        if (plan_kind(meta) != 3) continue;
+        int x, y;
+        if (w == 2)
+            ring2_xy(t, nx, ny, x, y);
+        else
+            ring1_xy(t, nx, ny, x, y);
+        double g[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)__ldg(pl + (1 + i) * R + t));
+        const double v = plan_combine(meta, g);
+        if (T) T[G.c(0, x, y)] = v;
+        s.C[G.c(n, x, y)] = v;
+    }
+}
+// The same for the h and g planes staged in As ([field][q][pool plane
+// layout]): one thread per (ghost cell, population), both fields.
+template <int N>
+__device__ void c2f_cells_hg(const DevState& s, const Geo<N>& G, int c, int n, double* As) {
+    const int nx = G.nx, ny = G.ny, RG = ring1_len(nx, ny), FP = 9 * G.aplane;
+    const int* pl = s.plan_hg + (size_t)c * RG * PLAN_INTS;
+    for (int idx = threadIdx.x; idx < 9 * RG; idx += blockDim.x) {
+        const int r = idx % RG, qq = idx / RG;
+        const int meta = __ldg(pl + r);
+        if (plan_kind(meta) != 3) continue;
+        int x, y;
+        ring1_xy(r, nx, ny, x, y);
+        unsigned o[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) o[i] = (unsigned)__ldg(pl + (1 + i) * RG + r) + qq * G.aplane;
+#pragma unroll
+        for (int f = 0; f < 2; ++f) {
+            double* A = f ? s.Ag : s.Ah;
+            double g[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) g[i] = __ldg(A + o[i]);
+            const double v = plan_combine(meta, g);
+            As[f * FP + G.a(0, qq + 1, x, y)] = v;
+            A[G.a(n, qq + 1, x, y)] = v;
+        }
+    }
+}
+
 __host__ __device__ constexpr int fill_c_min_blocks(int consumer) {
     return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) ? 2 : 3;
 }
@@ -654,17 +834,43 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     __shared__ int s_next;
     const int t = threadIdx.x;
     const int total = s.lvl_off[AMR_MAXLV];
-    fill_phase(
-        s, q, nbis, &s_next,
-        [&](int k, int n, const NbInfo& nbi) {
-            fill_c_ring<N>(s, G, k, n, w, 0);
-            if (nbi.c1[0]) {
-                wait_coarse(s, q, nbi);
-                fill_c_ring<N>(s, G, k, n, w, 1);
+    // fast: k_fill_flat has filled every ring; the walls are left to the
+    // consumer items. Else the fill phase fills level by level, walls included.
+    const bool fast = flat_fill(s, q);
+    if (!fast)
+        fill_phase(
+            s, q, nbis, &s_next,
+            [&](int k, int n, const NbInfo& nbi) {
+                if (nbi.wait) {
+                    fill_c_ring<N>(s, G, k, n, w, 1);
+                    wait_coarse(s, q, nbi);
+                    fill_c_ring<N>(s, G, k, n, w, 2);
+                } else {
+                    fill_c_ring<N>(s, G, k, n, w, 0);
+                }
+            },
+            [&](int n, const NbInfo& nbi) { wall_c<N>(s, G, n, nbi, w); });
+    // item c's level (record word lev[0]) and walls (id[3], id[4] < 0)
+    auto rec_walls = [&](int c, int& L, bool& w3, bool& w4) {
+        const int* rec = s.nbinfo + (size_t)c * NBI_STRIDE;
+        L = __ldg(rec + 9);
+        w3 = __ldg(rec + 3) < 0;
+        w4 = __ldg(rec + 4) < 0;
+    };
+    if (CONSUMER == CONS_NONE) {  // flat path: coarse-to-fine cells and walls in memory
+        if (fast)
+            for (int c = blockIdx.x; c < total; c += gridDim.x) {
+                int L;
+                bool w3, w4;
+                rec_walls(c, L, w3, w4);
+                const int n = __ldg(s.lvl_leaf + c);
+                c2f_cells_c<N>(s, G, c, n, w, nullptr);
+                __syncthreads();
+                if (w3 || w4) wall_c_rows<N>(s, G, n, w, w3, w4, nullptr);
+                __syncthreads();
             }
-        },
-        [&](int n, const NbInfo& nbi) { wall_c<N>(s, G, n, nbi, w); });
-    if (CONSUMER == CONS_NONE) return;
+        return;
+    }
 
     constexpr bool collide = (CONSUMER == CONS_COLLIDE_READ || CONSUMER == CONS_COLLIDE_FUSED);
     if (collide && blockIdx.x == 0 && t == 0)
@@ -677,7 +883,9 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     // without `block` only if it is done already (returns whether it started)
     auto start_tile = [&](int st, int c, bool block) {
         const int nn = __ldg(s.lvl_leaf + c);
-        if (block) {
+        if (fast) {
+            // the ring was written by the previous launch
+        } else if (block) {
             if (!spin_flag(flags + nn)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
         } else if (ld_acquire_i(flags + nn) == 0) {
             return false;
@@ -713,7 +921,18 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
             s_next = (int)cn;
             pend = ((int)cn < total) && !start_tile(st ^ 1, (int)cn, false);
         }
-        const double* T = tiles + (size_t)st * G.cplane;
+        double* T = tiles + (size_t)st * G.cplane;
+        if (fast) {  // coarse-to-fine cells, then Symmetric_C(2)_3/4, on the tile and in memory
+            int L;
+            bool w3, w4;
+            rec_walls(c, L, w3, w4);
+            c2f_cells_c<N>(s, G, c, n, w, T);
+            __syncthreads();
+            if (w3 || w4) {
+                wall_c_rows<N>(s, G, n, w, w3, w4, T);
+                __syncthreads();
+            }
+        }
         if (CONSUMER == CONS_MACRO_G)
             err_reduce(s, n, macro_g_block<N>(s, G, n, T), red);
         else
@@ -727,16 +946,15 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
 
 // ---------------------------------------------------------------------------
 // h/g ghost ring of the item at work position k (block n) from its plans,
-// into memory. pass 0: every cell that reads no coarser ring; pass 1: the
-// coarse-to-fine cells. A cell without a plan keeps its value in memory.
-// Copies take one thread per (ring cell, field) with the 9 populations' loads
-// in flight together; interpolated cells one thread per (ring cell, field,
-// population) with the 9 stencil loads in flight together.
+// into memory (mode as fill_c_ring). A cell without a plan keeps its value in
+// memory. Copies take one thread per (ring cell, field) with the 9
+// populations' loads in flight together; interpolated cells one thread per
+// (ring cell, field, population) with the 9 stencil loads in flight together.
 template <int N>
-__device__ void fill_hg_ring(const DevState& s, const Geo<N>& G, int k, int n, int pass) {
+__device__ void fill_hg_ring(const DevState& s, const Geo<N>& G, int k, int n, int mode) {
     const int nx = G.nx, ny = G.ny, RG = ring1_len(nx, ny);
     const int* pl = s.plan_hg + (size_t)k * RG * PLAN_INTS;
-    if (pass == 0) {
+    if (mode != 2) {
         for (int idx = threadIdx.x; idx < 2 * RG; idx += blockDim.x) {
             const int r = idx % RG;
             const int kind = plan_kind(__ldg(pl + r));
@@ -756,21 +974,23 @@ __device__ void fill_hg_ring(const DevState& s, const Geo<N>& G, int k, int n, i
             for (int qq = 0; qq < 9; ++qq) A[G.a(n, qq + 1, x, y)] = v[qq];
         }
     }
-    const int want = pass == 0 ? 2 : 3;
     for (int idx = threadIdx.x; idx < 18 * RG; idx += blockDim.x) {
         const int r = idx % RG, fq = idx / RG;
         const int meta = __ldg(pl + r);
-        if (plan_kind(meta) != want) continue;
+        const int kind = plan_kind(meta);
+        if (kind < 2 || !pass_takes(mode, kind)) continue;
         int x, y;
         ring1_xy(r, nx, ny, x, y);
         const int qq = fq % 9;
         double* A = (fq >= 9) ? s.Ag : s.Ah;
         const size_t qo = (size_t)qq * G.aplane;
         double g[9];
+        if (kind == 2) {
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            const double* src = A + (unsigned)__ldg(pl + (1 + i) * RG + r) + qo;
-            g[i] = (want == 3) ? ldcg(src) : __ldg(src);
+            for (int i = 0; i < 9; ++i) g[i] = __ldg(A + (unsigned)__ldg(pl + (1 + i) * RG + r) + qo);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) g[i] = ldcg(A + (unsigned)__ldg(pl + (1 + i) * RG + r) + qo);
         }
         A[G.a(n, qq + 1, x, y)] = plan_combine(meta, g);
     }
@@ -797,6 +1017,30 @@ __device__ void bounce_back(const DevState& s, const Geo<N>& G, int n, const NbI
             const double* src = A + G.a(n, J, Xn, Yi);
             A[G.a(n, i, X, Y)] = (Xn == 0 || Xn == nx + 1) ? ldcg(src) : __ldg(src);
         }
+    }
+}
+
+// The same walls on a block's h and g planes staged in shared memory (As:
+// [field][q][pool plane layout]), also written to memory. No barrier inside:
+// wall rows are written, rows 1 and ny read.
+template <int N>
+__device__ void bounce_back_staged(const DevState& s, const Geo<N>& G, int n, bool w3, bool w4,
+                                   double* As) {
+    const int nx = G.nx, ny = G.ny, FP = 9 * G.aplane;
+    for (int idx = threadIdx.x; idx < (nx + 2) * 36; idx += blockDim.x) {
+        const int X = idx % (nx + 2), qf = (idx / (nx + 2)) % 18;
+        const bool top = idx >= (nx + 2) * 18;
+        if (top ? !w4 : !w3) continue;
+        const int Y = top ? ny + 1 : 0, Yi = top ? ny : 1, sgn = top ? -1 : 1;
+        const int i = qf % 9 + 1, f = qf / 9;
+        int J = 1, Xn = X;
+        if (i > 1) {
+            Xn = min(max(0, X + sgn * d_ex(i) * d_ey(i)), nx + 1);
+            J = (i - 2) + 4 * ((i / 2) % 2);
+        }
+        const double v = As[f * FP + G.a(0, J, Xn, Yi)];
+        As[f * FP + G.a(0, i, X, Y)] = v;
+        (f ? s.Ag : s.Ah)[G.a(n, i, X, Y)] = v;
     }
 }
 
@@ -850,16 +1094,22 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s) {
     const int q = Q_FILLHG;
     const int t = threadIdx.x;
     const int total = s.lvl_off[AMR_MAXLV];
-    fill_phase(
-        s, q, nbis, &s_next,
-        [&](int k, int n, const NbInfo& nbi) {
-            fill_hg_ring<N>(s, G, k, n, 0);
-            if (nbi.c1[0]) {
-                wait_coarse(s, q, nbi);
-                fill_hg_ring<N>(s, G, k, n, 1);
-            }
-        },
-        [&](int n, const NbInfo& nbi) { bounce_back<N>(s, G, n, nbi); });
+    // fast: k_fill_flat has filled every ring; bounce-back is left to the
+    // streaming items. Else the fill phase fills level by level, walls included.
+    const bool fast = flat_fill(s, q);
+    if (!fast)
+        fill_phase(
+            s, q, nbis, &s_next,
+            [&](int k, int n, const NbInfo& nbi) {
+                if (nbi.wait) {
+                    fill_hg_ring<N>(s, G, k, n, 1);
+                    wait_coarse(s, q, nbi);
+                    fill_hg_ring<N>(s, G, k, n, 2);
+                } else {
+                    fill_hg_ring<N>(s, G, k, n, 0);
+                }
+            },
+            [&](int n, const NbInfo& nbi) { bounce_back<N>(s, G, n, nbi); });
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw);
     double* As = reinterpret_cast<double*>(smraw + 128);  // [h|g][q][pool plane layout]
     const int FP = 9 * G.aplane;
@@ -877,7 +1127,7 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s) {
         const int n = __ldg(s.lvl_leaf + c);
         if (t == 0) {
             cn = atomicAdd(&s.queue[2 * q + 1], 1u);
-            if (!spin_flag(flags + n)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
+            if (!fast && !spin_flag(flags + n)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
             fence_proxy_async_all();
             mbar_expect_tx(bar, 2 * fb);
             bulk_g2s(As, s.Ah + (size_t)n * FP, fb, bar);
@@ -890,6 +1140,16 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s) {
             break;
         }
         phase ^= 1u;
+        if (fast) {  // coarse-to-fine cells, then Bounce_Back_3/4, on the staged planes and in memory
+            const int* rec = s.nbinfo + (size_t)c * NBI_STRIDE;
+            const bool w3 = __ldg(rec + 3) < 0, w4 = __ldg(rec + 4) < 0;
+            c2f_cells_hg<N>(s, G, c, n, As);
+            __syncthreads();
+            if (w3 || w4) {
+                bounce_back_staged<N>(s, G, n, w3, w4, As);
+                __syncthreads();
+            }
+        }
         stream_block<N>(s, G, n, As);
         c = s_next;
         __syncthreads();
@@ -1032,6 +1292,7 @@ int queue_grid(K kernel, int nt, size_t smem, const LaunchCfg& lc) {
     return lc.num_sms * occ;
 }
 
+// shared memory of a C-fill launch: mbarriers, two C tiles
 size_t fill_c_smem(const DevState& s) { return 128 + 2 * sizeof(double) * (size_t)s.cplane; }
 
 template <int N, int CONS>
@@ -1069,6 +1330,14 @@ void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int 
     cudaMemsetAsync(s.queue + 2 * q, 0, 2 * sizeof(unsigned), st);
     cudaMemsetAsync(s.ring_done + (size_t)q * (s.max_blks + 1), 0,
                     sizeof(int) * (size_t)(s.max_blks + 1), st);
+#define F_(N)                                                      \
+    if (width == 2)                                                \
+        k_fill_flat<N, Q_FILLC><<<lc.num_sms * 8, 256, 0, st>>>(s);  \
+    else                                                           \
+        k_fill_flat<N, Q_FILLC1><<<lc.num_sms * 8, 256, 0, st>>>(s)
+    DISPATCH(s, F_);
+#undef F_
+    count_launches(1);
 #define C_(N) fill_c_dispatch<N>(s, lc, st, width, consumer, q)
     DISPATCH(s, C_);
 #undef C_
@@ -1079,8 +1348,12 @@ void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t 
     cudaMemsetAsync(s.queue + 2 * Q_FILLHG, 0, 2 * sizeof(unsigned), st);
     cudaMemsetAsync(s.ring_done + (size_t)Q_FILLHG * (s.max_blks + 1), 0,
                     sizeof(int) * (size_t)(s.max_blks + 1), st);
+#define F_(N) k_fill_flat<N, Q_FILLHG><<<lc.num_sms * 8, 256, 0, st>>>(s)
+    DISPATCH(s, F_);
+#undef F_
+    count_launches(1);
     const int nt = block_threads(s);
-    const size_t sm = 128 + 18 * sizeof(double) * (size_t)s.aplane;
+    const size_t sm = 128 + 18 * sizeof(double) * (size_t)s.aplane;  // mbarrier, h and g planes
 #define C_(N)                                                                            \
     smem_optin(k_fill_hg_stream<N>, sm);                                                 \
     k_fill_hg_stream<N><<<queue_grid(k_fill_hg_stream<N>, nt, sm, lc), nt, sm, st>>>(s)
@@ -1090,6 +1363,7 @@ void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t 
 }
 
 void launch_build_plans(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+    cudaMemsetAsync(s.fillinfo, 0, 3 * NQUEUES * sizeof(int), st);
 #define C_(N) k_build_plans<N><<<lc.grid_leaves, 128, 0, st>>>(s)
     DISPATCH(s, C_);
 #undef C_
