@@ -285,11 +285,12 @@ void enqueue_step(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail, bo
     const DevState& s = ctx->s;
     {
         ProfMark m(ctx, ge, 0);
-        launch_fill_c(s, ctx->lc, ctx->st, 2, prev_tail ? CONS_COLLIDE_READ : CONS_COLLIDE_FUSED);
+        launch_fill_c(s, ctx->lc, ctx->st, 2, prev_tail ? CONS_COLLIDE_READ : CONS_COLLIDE_FUSED,
+                      last ? 1 : 0);
     }
     {
         ProfMark m(ctx, ge, 1);
-        launch_fill_hg_stream(s, ctx->lc, ctx->st);
+        launch_fill_hg_stream(s, ctx->lc, ctx->st, last ? 1 : 0);
     }
     if (tail) {
         ProfMark m(ctx, ge, 2);
@@ -473,10 +474,12 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     AL(plan_c2, int, NB * PLAN_INTS * (size_t)(4 * (nx + ny) + 16));
     AL(plan_c1, int, NB * PLAN_INTS * (size_t)(2 * (nx + ny) + 4));
     AL(plan_hg, int, NB * PLAN_INTS * (size_t)(2 * (nx + ny) + 4));
-    AL(fillinfo, int, 3 * NQUEUES);
-    AL(interp_c2, int, 2 * NB * (size_t)(4 * (nx + ny) + 16));
-    AL(interp_c1, int, 2 * NB * (size_t)(2 * (nx + ny) + 4));
-    AL(interp_hg, int, 2 * NB * (size_t)(2 * (nx + ny) + 4));
+    // a fine leaf reads at most half a side plus two cells of a coarser
+    // neighbour's ring per side, and five cells per corner
+    s.fmax = 2 * (nx > ny ? nx : ny) + 28;
+    AL(frn_c, int, NB * 11 * (size_t)s.fmax);
+    AL(frn_hg, int, NB * 11 * (size_t)s.fmax);
+    AL(fillinfo, int, NQUEUES);
     AL(freelist, int, (size_t)s.fl_cap);
     AL(ref_list, int, NB);
     AL(ref_c1, int, NB);

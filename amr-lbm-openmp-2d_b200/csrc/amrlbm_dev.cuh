@@ -78,13 +78,9 @@ struct DevState {
     int *lvl_off;    // lvl_off[AMR_MAXLV] = number of entries of lvl_leaf
     int *nbinfo;     // [k][NBI_STRIDE] neighbour record of lvl_leaf[k]
     int *plan_c2, *plan_c1, *plan_hg;  // [k][PLAN_INTS][ring] fill plans of lvl_leaf[k]
-    // [q]: a fill of queue q needs level order; [NQUEUES+q], [2*NQUEUES+q]:
-    // copied and fine-to-coarse ghost cells of that fill
-    int* fillinfo;
-    // units of the flat fills, 2 ints each in 2*(max_blks+1)*R ints: copies
-    // (dest, source offset) from the front, fine-to-coarse cells (dest,
-    // k*R + t) from the back
-    int *interp_c2, *interp_c1, *interp_hg;
+    int *frn_c, *frn_hg;               // [k][11][fmax] foreign cells (C / A offsets)
+    int fmax;                          // foreign cells per leaf and fill, at most
+    int* fillinfo;                     // [q]: fill q needs level order
     int *freelist;   // ring buffer of the first ids of freed quartets
     int *ref_list, *ref_c1, *der_list;
     Counters* cnt;

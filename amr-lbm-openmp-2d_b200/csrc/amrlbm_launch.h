@@ -19,9 +19,14 @@ struct LaunchCfg {
     int grid_leaves;    // CTAs of a grid-stride kernel over leaves
 };
 
+// write_ring: without level order, the consumer items write the ghost rings
+// they fill to memory only if set (their own launch reads them from shared
+// memory; the state after a step holds them); fills with level order and
+// CONS_NONE always write them
 void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width,
-                   int consumer);
-void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+                   int consumer, int write_ring = 1);
+void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st,
+                           int write_ring = 1);
 void launch_collide(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_macro_h(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_macro_g(const DevState& s, const LaunchCfg& lc, cudaStream_t st);

@@ -7,16 +7,18 @@
 // level by level (Fill_Ghost_Cells_C.f90:8-38): a coarse-to-fine fill reads
 // the coarse neighbour's ghost ring, written one level earlier. Here, after
 // every topology change, each ghost cell of each leaf gets a fill plan (copy,
-// fine-to-coarse or coarse-to-fine interpolation, with its source offsets).
-// When every coarse-to-fine source is an interior cell or a coarser
-// neighbour's ghost cell that is itself a copy or a fine-to-coarse value (the
-// usual case), two flat launches fill all rings: copies and fine-to-coarse
-// cells first, coarse-to-fine cells second; the consumer launch (collision,
-// streaming or macroscopic values) applies the walls. Otherwise the consumer
-// launch fills level by level first: CTAs claim leaves from a queue in which
-// every leaf a finer neighbour reads precedes its readers, a leaf waits
-// (bounded spin) for its coarser neighbours' flags, and no grid barrier is
-// needed.
+// fine-to-coarse or coarse-to-fine interpolation, with its source offsets);
+// a coarser neighbour's ghost cell that a coarse-to-fine stencil reads and
+// that is itself a copy or a fine-to-coarse value becomes a "foreign" cell of
+// the reader, evaluated by the reader from interiors. Then every leaf's ring
+// depends on interiors only (the usual case): each consumer item (collision,
+// streaming or macroscopic values of one leaf) fills its own ring on its
+// staged tile, applies the walls and consumes, with no ordering between
+// leaves. Otherwise the consumer launch fills level by level first: CTAs
+// claim leaves from a queue in which every leaf a finer neighbour reads
+// precedes its readers, a leaf waits (bounded spin) for the flags of the
+// coarser neighbours it reads, and no grid barrier is needed.
+#include <cstddef>
 #include <cstdio>
 
 #include "amrlbm_fast.cuh"
@@ -47,12 +49,13 @@ __device__ __forceinline__ int ghost_dir(int x, int y, int nx, int ny) {
 
 // per-direction neighbour data of the block being filled, loaded once into
 // shared memory: resolved id, its level, leaf flag and first child (index 0:
-// the block itself); wait: the directions of coarser neighbours, whose rings
-// a level-ordered fill waits for
+// the block itself); per fill q: wait[q], the directions whose rings a
+// level-ordered fill waits for, and nf[q], the number of foreign cells
 struct NbInfo {
     int id[9], lev[9], leaf[9], c1[9];
     int bi, bj;
-    int wait;
+    int wait[NQUEUES];
+    int nf[NQUEUES];
 };
 constexpr int NBI_INTS = (int)(sizeof(NbInfo) / sizeof(int));
 static_assert(NBI_INTS <= NBI_STRIDE, "NbInfo record");
@@ -220,6 +223,22 @@ __host__ __device__ __forceinline__ int ring1_len(int nx, int ny) { return 2 * (
 
 
 // ---------------------------------------------------------------------------
+// Source word of a packed plan: bit 31 clear: offset (doubles) of the source
+// in the pool array; set: slot of a foreign cell of the item, a coarser
+// neighbour's ghost cell that is a copy or a fine-to-coarse value of
+// interiors, which the item evaluates itself before its coarse-to-fine
+// cells. A foreign record (FRN_INTS ints, plane by plane over fmax slots)
+// holds that ghost cell's plan (meta word, 9 sources) and its offset.
+constexpr unsigned kIndirect = 0x80000000u;
+constexpr int FRN_INTS = 11;
+
+__device__ __forceinline__ int ring1_index(int x, int y, int nx, int ny) {
+    if (y == 0) return x;
+    if (y == ny + 1) return nx + 2 + x;
+    return 2 * (nx + 2) + (x == 0 ? 0 : ny) + (y - 1);
+}
+
+// ---------------------------------------------------------------------------
 // Neighbour records and fill plans of every leaf, in work order (one CTA per
 // leaf). The neighbour data is what Fill_Ghost_Cells_* reads through the
 // block pointers (Fill_Ghost_Cells_C.f90:8-38): resolved neighbour ids, their
@@ -227,12 +246,13 @@ __host__ __device__ __forceinline__ int ring1_len(int nx, int ny) { return 2 * (
 // ring_out flag.
 //
 // Coarse-to-fine cells read the coarser neighbour's ring, which the
-// reference fills one level earlier. Where such a ring cell is itself a copy
-// or a fine-to-coarse interpolation of interiors, the plan refers to that
-// cell's own plan entry and the fill evaluates it in place, with the same
-// operations the neighbour's fill uses, so the fill need not wait. Only where
-// it is a coarse-to-fine or wall cell does the record's wait mask make the
-// fill wait for the neighbour's flag.
+// reference fills one level earlier. Where such a ring cell is a copy or a
+// fine-to-coarse value, it becomes a foreign cell of the reading leaf: the
+// leaf evaluates it from its plan, with the operations the neighbour's own
+// fill uses, so the two leaves need not be ordered. Where it is itself
+// coarse-to-fine or a wall cell, or a fill meets a level jump, the fill is
+// marked as needing level order (fillinfo[q]), and the record's wait mask
+// names the neighbours whose rings the leaf waits for then.
 __device__ void load_nbinfo(const DevState& s, int n, NbInfo& r) {
     for (int j = 0; j < 8; ++j) {
         const int b = s.nbr[8 * n + j];
@@ -247,75 +267,138 @@ __device__ void load_nbinfo(const DevState& s, int n, NbInfo& r) {
     r.c1[0] = 0;
     r.bi = s.bi[n];
     r.bj = s.bj[n];
-    r.wait = 0;
+    for (int q = 0; q < NQUEUES; ++q) r.wait[q] = r.nf[q] = 0;
 }
 
+// One pass over the ghost cells of rings 1-2 serves all three fills: a cell's
+// plan is the same in the C2, C1 and h/g fills (only the offsets differ, C
+// pool or A pool), and a leaf's foreign cells are shared by the three.
 template <int N>
 __global__ void k_build_plans(DevState s) {
     const Geo<N> G(s);
+    extern __shared__ int tab[];  // [9][ring1_len]: foreign cell -> slot
     __shared__ NbInfo nbi;
-    __shared__ NbInfo cnb[9];  // coarser neighbours' records
+    __shared__ NbInfo cnb[9];     // coarser neighbours' records
+    __shared__ int nfs;
     const int nx = G.nx, ny = G.ny, R2 = ring2_len(nx, ny), R1 = ring1_len(nx, ny);
     const int total = s.lvl_off[AMR_MAXLV];
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, fmax = s.fmax;
     for (int k = blockIdx.x; k < total; k += gridDim.x) {
         const int n = s.lvl_leaf[k];
-        if (t == 0) load_nbinfo(s, n, nbi);
+        if (t == 0) {
+            load_nbinfo(s, n, nbi);
+            nfs = 0;
+        }
+        for (int i = t; i < 9 * R1; i += blockDim.x) tab[i] = -1;
         __syncthreads();
         const int L = nbi.lev[0];
-        if (t >= 1 && t <= 8 && nbi.id[t] > 0 && nbi.lev[t] == L - 1) {
-            load_nbinfo(s, nbi.id[t], cnb[t]);
-            atomicOr(&nbi.wait, 1 << t);
-        }
+        if (t >= 1 && t <= 8 && nbi.id[t] > 0 && nbi.lev[t] == L - 1) load_nbinfo(s, nbi.id[t], cnb[t]);
         __syncthreads();
-        // one plan type: queue q, plan array, unit lists of the flat fill
-        // (copies (dest, source) from the front, fine-to-coarse cells (dest,
-        // k*R + t) from the back, 2 ints each), ring length R, ring-2
-        // indexing, offsets into the A pool (else C)
-        auto build = [&](int q, int* plans, int* units, int R, bool two, bool afield) {
-            auto off = [&](int blk, int xx, int yy) -> long long {
-                return afield ? (long long)G.a(blk, 1, xx, yy) : (long long)G.c(blk, xx, yy);
-            };
-            const size_t cap2 = 2 * (size_t)(s.max_blks + 1) * R;
-            for (int i = t; i < R; i += blockDim.x) {
-                int x, y;
-                if (two)
-                    ring2_xy(i, nx, ny, x, y);
-                else
-                    ring1_xy(i, nx, ny, x, y);
-                const int d = ghost_dir(x, y, nx, ny);
-                bool deep = false;
-                GPlan P;
-                ghost_plan(nbi, nx, ny, L, d, x, y,
-                           [&](int blk, int xx, int yy) -> long long {
-                               // a coarser neighbour's ghost cell must be a copy or
-                               // a fine-to-coarse value (its neighbour on that
-                               // side exists and has its level) for the flat fill
-                               const bool ring = xx < 1 || xx > nx || yy < 1 || yy > ny;
-                               if (ring && blk == nbi.id[d] && nbi.lev[d] == L - 1) {
-                                   const int dd = ghost_dir(xx, yy, nx, ny);
-                                   if (!nbi.leaf[d] || cnb[d].id[dd] <= 0 || cnb[d].lev[dd] != L - 1)
-                                       deep = true;
+        auto offc = [&](int blk, int xx, int yy) -> long long { return (long long)G.c(blk, xx, yy); };
+        // ghost cell (xx,yy) of block blk, read from direction d: 1 a foreign
+        // cell (the coarser neighbour's neighbour on that side has its level:
+        // a copy or a fine-to-coarse value), -1 a coarser ring cell that is
+        // not, 0 not a coarser neighbour's ghost cell
+        auto foreign = [&](int d, int blk, int xx, int yy) {
+            const bool ring = xx < 1 || xx > nx || yy < 1 || yy > ny;
+            if (!ring || blk != nbi.id[d] || nbi.lev[d] != L - 1) return 0;
+            const int dd = ghost_dir(xx, yy, nx, ny);
+            return (nbi.leaf[d] && cnb[d].id[dd] > 0 && cnb[d].lev[dd] == L - 1) ? 1 : -1;
+        };
+        // 1: mark the foreign cells; anything else makes the fills wait
+        for (int i = t; i < R2; i += blockDim.x) {
+            int x, y;
+            ring2_xy(i, nx, ny, x, y);
+            const bool r1 = x >= 0 && x <= nx + 1 && y >= 0 && y <= ny + 1;
+            const int d = ghost_dir(x, y, nx, ny);
+            GPlan P;
+            ghost_plan(nbi, nx, ny, L, d, x, y,
+                       [&](int blk, int xx, int yy) -> long long {
+                           const int f = foreign(d, blk, xx, yy);
+                           if (f > 0) tab[d * R1 + ring1_index(xx, yy, nx, ny)] = -2;
+                           if (f < 0) {
+                               atomicOr(&nbi.wait[Q_FILLC], 1 << d);
+                               if (r1) {
+                                   atomicOr(&nbi.wait[Q_FILLC1], 1 << d);
+                                   atomicOr(&nbi.wait[Q_FILLHG], 1 << d);
                                }
-                               return off(blk, xx, yy);
-                           },
-                           P);
-                plan_store(plans + (size_t)k * R * PLAN_INTS, R, i, P);
-                if (deep || P.kind < 0) atomicOr(&s.fillinfo[q], 1);  // a level jump is reported there
-                if (P.kind == 1) {
-                    const size_t j = atomicAdd(&s.fillinfo[NQUEUES + q], 1);
-                    units[2 * j] = (int)off(n, x, y);
-                    units[2 * j + 1] = (int)(unsigned)P.src[0];
-                } else if (P.kind == 2) {
-                    const size_t j = atomicAdd(&s.fillinfo[2 * NQUEUES + q], 1);
-                    units[cap2 - 2 - 2 * j] = (int)off(n, x, y);
-                    units[cap2 - 1 - 2 * j] = k * R + i;
+                           }
+                           return 0;
+                       },
+                       P);
+            if (P.kind < 0) {  // the level jump is reported by the level-ordered fills
+                atomicOr(&s.fillinfo[Q_FILLC], 1);
+                if (r1) {
+                    atomicOr(&s.fillinfo[Q_FILLC1], 1);
+                    atomicOr(&s.fillinfo[Q_FILLHG], 1);
                 }
             }
-        };
-        build(Q_FILLC, s.plan_c2, s.interp_c2, R2, true, false);
-        build(Q_FILLC1, s.plan_c1, s.interp_c1, R1, false, false);
-        build(Q_FILLHG, s.plan_hg, s.interp_hg, R1, false, true);
+        }
+        __syncthreads();
+        // 2: number the marked cells and write their records (C and A offsets)
+        int* fc = s.frn_c + (size_t)k * fmax * FRN_INTS;
+        int* fa = s.frn_hg + (size_t)k * fmax * FRN_INTS;
+        for (int i = t; i < 9 * R1; i += blockDim.x) {
+            if (tab[i] != -2) continue;
+            const int j = atomicAdd(&nfs, 1);
+            tab[i] = j;
+            if (j >= fmax) {  // not reached: fmax bounds the cells a leaf reads
+                set_error(s, 7 /*AMRLBM_ERR_STATE*/, n);
+                continue;
+            }
+            const int d = i / R1;
+            int xx, yy;
+            ring1_xy(i % R1, nx, ny, xx, yy);
+            long long aoff[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            int na = 0;
+            GPlan sub;  // the coarser neighbour's plan of that ghost cell
+            ghost_plan(cnb[d], nx, ny, L - 1, ghost_dir(xx, yy, nx, ny), xx, yy,
+                       [&](int blk, int x2, int y2) -> long long {
+                           aoff[na++ % 9] = (long long)G.a(blk, 1, x2, y2);
+                           return offc(blk, x2, y2);
+                       },
+                       sub);
+            plan_store(fc, fmax, j, sub);
+            fc[10 * fmax + j] = (int)offc(nbi.id[d], xx, yy);
+            for (int m = 0; m < 9; ++m) sub.src[m] = aoff[m];
+            plan_store(fa, fmax, j, sub);
+            fa[10 * fmax + j] = (int)G.a(nbi.id[d], 1, xx, yy);
+        }
+        __syncthreads();
+        if (t < NQUEUES) {
+            nbi.nf[t] = nfs;
+            if (nbi.wait[t]) atomicOr(&s.fillinfo[t], 1);
+        }
+        // 3: the plans, foreign cells by slot
+        for (int i = t; i < R2; i += blockDim.x) {
+            int x, y;
+            ring2_xy(i, nx, ny, x, y);
+            const int d = ghost_dir(x, y, nx, ny);
+            long long aoff[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            int na = 0;
+            GPlan P;
+            ghost_plan(nbi, nx, ny, L, d, x, y,
+                       [&](int blk, int xx, int yy) -> long long {
+                           long long w, wa;
+                           if (foreign(d, blk, xx, yy) > 0) {
+                               w = wa = (long long)(kIndirect |
+                                                    (unsigned)tab[d * R1 + ring1_index(xx, yy, nx, ny)]);
+                           } else {
+                               w = offc(blk, xx, yy);
+                               wa = (long long)G.a(blk, 1, xx, yy);
+                           }
+                           aoff[na++ % 9] = wa;
+                           return w;
+                       },
+                       P);
+            plan_store(s.plan_c2 + (size_t)k * R2 * PLAN_INTS, R2, i, P);
+            if (x >= 0 && x <= nx + 1 && y >= 0 && y <= ny + 1) {
+                const int i1 = ring1_index(x, y, nx, ny);
+                plan_store(s.plan_c1 + (size_t)k * R1 * PLAN_INTS, R1, i1, P);
+                for (int m = 0; m < 9; ++m) P.src[m] = aoff[m];
+                plan_store(s.plan_hg + (size_t)k * R1 * PLAN_INTS, R1, i1, P);
+            }
+        }
         __syncthreads();
         if (t < NBI_STRIDE)
             s.nbinfo[(size_t)k * NBI_STRIDE + t] = (t < NBI_INTS) ? reinterpret_cast<int*>(&nbi)[t] : 0;
@@ -324,15 +407,16 @@ __global__ void k_build_plans(DevState s) {
 }
 
 // ---------------------------------------------------------------------------
-// Level-ordered launches: two phases in one launch.
-//
-// Fill phase: CTAs claim fill items (one leaf's ghost ring) in work order
-// from queue[2q]. A fill item that reads a coarser neighbour's ring waits
-// (bounded spin) for that neighbour's flag; every fill item raises its own
-// block's flag when its ring, walls included, is in memory. Consumer phase:
-// once the fill queue is empty, CTAs claim consumer items (the work that
-// needs the block's own ring: collision, streaming, macroscopic values) from
-// queue[2q+1]; a consumer item waits only for its own block's flag.
+// Level-ordered launches, for fills that need level order: two phases in
+// one launch. Fill phase: CTAs claim fill items (one leaf's ghost ring) in
+// work order from queue[2q]. A fill item whose coarse-to-fine cells read a
+// coarser neighbour's ring (other than its foreign cells) waits (bounded
+// spin) for that neighbour's flag; every fill item raises its own block's
+// flag when its ring, walls included, is in memory. Consumer phase: once the
+// fill queue is empty, CTAs claim consumer items (the work that needs the
+// block's own ring: collision, streaming, macroscopic values) from
+// queue[2q+1]; a consumer item waits only for its own block's flag. Without
+// level order there is no fill phase and consumer items fill their own rings.
 //
 // A CTA claims its next item as soon as it starts the current one (the
 // atomic's latency hides behind the work). Progress: the smallest unfinished
@@ -358,7 +442,7 @@ __device__ __forceinline__ bool spin_flag(const int* flag) {
 // block-uniform, ends with a barrier
 __device__ __forceinline__ void wait_coarse(const DevState& s, int q, const NbInfo& nbi) {
     const int t = threadIdx.x;
-    if (t < 8 && ((nbi.wait >> (t + 1)) & 1))
+    if (t < 8 && ((nbi.wait[q] >> (t + 1)) & 1))
         if (!spin_flag(fill_flags(s, q) + nbi.id[t + 1])) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, q);
     __syncthreads();
 }
@@ -420,7 +504,7 @@ __device__ __forceinline__ void fill_phase(const DevState& s, int q, NbInfo* nbi
 // then is the source. No barrier inside: the rows read and written differ.
 template <int N>
 __device__ void wall_c_rows(const DevState& s, const Geo<N>& G, int n, int w, bool w3, bool w4,
-                            double* T) {
+                            double* T, bool to_mem = true) {
     const int nx = G.nx, ny = G.ny;
     for (int idx = threadIdx.x; idx < (nx + 2 * w) * w * 2; idx += blockDim.x) {
         const int X = idx % (nx + 2 * w) + 1 - w, a = (idx / (nx + 2 * w)) % w + 1;
@@ -429,8 +513,65 @@ __device__ void wall_c_rows(const DevState& s, const Geo<N>& G, int n, int w, bo
         const int ys = top ? ny + 1 - a : a, yd = top ? ny + a : 1 - a;
         const double v = T ? T[G.c(0, X, ys)] : ldcg(s.C + G.c(n, X, ys));
         if (T) T[G.c(0, X, yd)] = v;
-        s.C[G.c(n, X, yd)] = v;
+        if (to_mem) s.C[G.c(n, X, yd)] = v;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Ghost values from the plans. A fill item first evaluates its foreign cells
+// into Fs (shared memory, Fs[plane * fmax + slot]), then its ghost cells.
+
+// Whether fill q runs without level order: no leaf's fill waits for a
+// coarser neighbour, no level jump, every leaf's level in [LevelMin,
+// LevelMax]. Then every fill item depends on interiors only.
+__device__ __forceinline__ bool fast_fill(const DevState& s, int q) {
+    return s.fillinfo[q] == 0 && s.cnt->level_min <= s.cnt->leaf_min &&
+           s.cnt->level_max >= s.cnt->leaf_max;
+}
+
+// Value of foreign cell j (records at fb) on the plane at qo of pool array A
+// (C, or the first plane of Ah / Ag). live: the coarser neighbour is filled
+// in this launch; if not, its ghost cell keeps the value in memory, as in the
+// reference.
+__device__ __forceinline__ double foreign_value(const int* fb, int fmax, int j, const double* A,
+                                                size_t qo, bool live) {
+    if (!live) return ldcg(A + (unsigned)__ldg(fb + 10 * fmax + j) + qo);
+    const int meta = __ldg(fb + j);
+    if (plan_kind(meta) == 1) return __ldg(A + (unsigned)__ldg(fb + fmax + j) + qo);
+    double g[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) g[i] = __ldg(A + (unsigned)__ldg(fb + (1 + i) * fmax + j) + qo);
+    return plan_combine(meta, g);
+}
+
+// foreign cells of item k of a C fill (w: ring width) into Fs; ends with a
+// barrier when there are any (nf is block-uniform)
+template <int N>
+__device__ void foreign_c(const DevState& s, int k, int w, int nf, bool live, double* Fs) {
+    if (nf == 0) return;
+    const int* fb = s.frn_c + (size_t)k * s.fmax * FRN_INTS;
+    for (int j = threadIdx.x; j < nf; j += blockDim.x) Fs[j] = foreign_value(fb, s.fmax, j, s.C, 0, live);
+    __syncthreads();
+}
+// the same for the h/g fill: one thread per (slot, field and population)
+template <int N>
+__device__ void foreign_hg(const DevState& s, const Geo<N>& G, int k, int nf, bool live,
+                           double* Fs) {
+    if (nf == 0) return;
+    const int* fb = s.frn_hg + (size_t)k * s.fmax * FRN_INTS;
+    for (int idx = threadIdx.x; idx < 18 * nf; idx += blockDim.x) {
+        const int j = idx % nf, fq = idx / nf;
+        Fs[fq * s.fmax + j] = foreign_value(fb, s.fmax, j, (fq >= 9) ? s.Ag : s.Ah,
+                                            (size_t)(fq % 9) * G.aplane, live);
+    }
+    __syncthreads();
+}
+
+// a coarse-to-fine source: a foreign slot's value in Fs, or a cell in memory
+// (the coarser neighbour's interior, or its ring after a wait: through L2)
+__device__ __forceinline__ double c2f_source(unsigned w, const double* Fs, const double* A,
+                                             size_t qo) {
+    return (w & kIndirect) ? Fs[w & ~kIndirect] : ldcg(A + w + qo);
 }
 
 // which plan kinds a fill pass evaluates: 0 all, 1 all but coarse-to-fine
@@ -439,12 +580,13 @@ __device__ __forceinline__ bool pass_takes(int mode, int kind) {
     return mode == 0 || ((kind == 3) == (mode == 2));
 }
 
-// C ghost ring of width w of the item at work position k (block n) from its
-// plans, into memory (level-ordered path). Kind 1 and 2 sources are
-// interiors nothing writes during the launch; kind 3 sources include a
-// coarser neighbour's ring written in it (read through L2 after the wait).
+// C ghost ring of width w of item k (block n) from its plans, into memory
+// (unless to_mem is false) and, if T is given, into the block's shared C tile
+// (index G.c(0,x,y)). Kind 1 and 2 sources are interiors no launch of this
+// fill writes.
 template <int N>
-__device__ void fill_c_ring(const DevState& s, const Geo<N>& G, int k, int n, int w, int mode) {
+__device__ void fill_ring_c(const DevState& s, const Geo<N>& G, int k, int n, int w, int mode,
+                            const double* Fs, double* T, bool to_mem = true) {
     const int nx = G.nx, ny = G.ny;
     const int R = (w == 2) ? ring2_len(nx, ny) : ring1_len(nx, ny);
     const int* pl = ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)k * R * PLAN_INTS;
@@ -471,11 +613,76 @@ __device__ void fill_c_ring(const DevState& s, const Geo<N>& G, int k, int n, in
                 for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)__ldg(pl + (1 + i) * R + t));
             } else {
 #pragma unroll
-                for (int i = 0; i < 9; ++i) g[i] = ldcg(s.C + (unsigned)__ldg(pl + (1 + i) * R + t));
+                for (int i = 0; i < 9; ++i)
+                    g[i] = c2f_source((unsigned)__ldg(pl + (1 + i) * R + t), Fs, s.C, 0);
             }
             v = plan_combine(meta, g);
         }
-        s.C[G.c(n, x, y)] = v;
+        if (to_mem) s.C[G.c(n, x, y)] = v;
+        if (T) T[G.c(0, x, y)] = v;
+    }
+}
+
+// h/g ghost ring of item k (block n) from its plans, into memory (unless
+// to_mem is false) and, if As is given, into the block's staged planes
+// ([field][q][pool plane layout]).
+// A cell without a plan keeps its value in memory. Copies take one thread per
+// (ghost cell, field) with the 9 populations' loads in flight together;
+// interpolated cells one thread per (ghost cell, population), both fields.
+template <int N>
+__device__ void fill_ring_hg(const DevState& s, const Geo<N>& G, int k, int n, int mode,
+                             const double* Fs, double* As, bool to_mem = true) {
+    const int nx = G.nx, ny = G.ny, RG = ring1_len(nx, ny), FP = 9 * G.aplane;
+    const int* pl = s.plan_hg + (size_t)k * RG * PLAN_INTS;
+    if (mode != 2) {
+        for (int idx = threadIdx.x; idx < 2 * RG; idx += blockDim.x) {
+            const int r = idx % RG, f = idx / RG;
+            const int kind = plan_kind(__ldg(pl + r));
+            if (kind != 1 && kind != -1) continue;
+            int x, y;
+            ring1_xy(r, nx, ny, x, y);
+            if (kind < 0) {
+                set_error(s, 4 /*AMRLBM_ERR_LEVEL_JUMP*/, n);
+                continue;
+            }
+            double* A = f ? s.Ag : s.Ah;
+            const double* src = A + (unsigned)__ldg(pl + RG + r);
+            double v[9];
+#pragma unroll
+            for (int qq = 0; qq < 9; ++qq) v[qq] = __ldg(src + (size_t)qq * G.aplane);
+#pragma unroll
+            for (int qq = 0; qq < 9; ++qq) {
+                if (to_mem) A[G.a(n, qq + 1, x, y)] = v[qq];
+                if (As) As[f * FP + G.a(0, qq + 1, x, y)] = v[qq];
+            }
+        }
+    }
+    for (int idx = threadIdx.x; idx < 9 * RG; idx += blockDim.x) {
+        const int r = idx % RG, qq = idx / RG;
+        const int meta = __ldg(pl + r);
+        const int kind = plan_kind(meta);
+        if (kind < 2 || !pass_takes(mode, kind)) continue;
+        int x, y;
+        ring1_xy(r, nx, ny, x, y);
+        const size_t qo = (size_t)qq * G.aplane;
+        unsigned wd[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) wd[i] = (unsigned)__ldg(pl + (1 + i) * RG + r);
+#pragma unroll
+        for (int f = 0; f < 2; ++f) {
+            double* A = f ? s.Ag : s.Ah;
+            double g[9];
+            if (kind == 2) {
+#pragma unroll
+                for (int i = 0; i < 9; ++i) g[i] = __ldg(A + wd[i] + qo);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 9; ++i) g[i] = c2f_source(wd[i], Fs + (f * 9 + qq) * s.fmax, A, qo);
+            }
+            const double v = plan_combine(meta, g);
+            if (to_mem) A[G.a(n, qq + 1, x, y)] = v;
+            if (As) As[f * FP + G.a(0, qq + 1, x, y)] = v;
+        }
     }
 }
 
@@ -701,301 +908,6 @@ __device__ __forceinline__ void err_reduce(const DevState& s, int n, double mx, 
     }
 }
 
-// ---------------------------------------------------------------------------
-// Whether fill Q takes the flat path: no coarse-to-fine cell reads a coarser
-// neighbour's ghost cell that is itself coarse-to-fine or a wall cell, and
-// every leaf's level is in [LevelMin, LevelMax]. Else the consumer launch
-// fills level by level.
-__device__ __forceinline__ bool flat_fill(const DevState& s, int q) {
-    return s.fillinfo[q] == 0 && s.cnt->level_min <= s.cnt->leaf_min &&
-           s.cnt->level_max >= s.cnt->leaf_max;
-}
-
-// The copies and fine-to-coarse ghost cells of every leaf, one flat launch:
-// one thread per copied cell (and field: its 9 populations together), one per
-// fine-to-coarse cell (and field and population). Every source is an
-// interior cell no launch of this fill writes. The coarse-to-fine cells (which
-// read the copies and fine-to-coarse cells of coarser neighbours) and the
-// walls are left to the consumer launch.
-template <int N, int Q>
-__global__ void __launch_bounds__(256) k_fill_flat(DevState s) {
-    if (!flat_fill(s, Q)) return;
-    const Geo<N> G(s);
-    constexpr bool HG = (Q == Q_FILLHG);
-    constexpr int F = HG ? 2 : 1;
-    const int R = (Q == Q_FILLC) ? ring2_len(G.nx, G.ny) : ring1_len(G.nx, G.ny);
-    const int* plans = (Q == Q_FILLC) ? s.plan_c2 : (Q == Q_FILLC1 ? s.plan_c1 : s.plan_hg);
-    const int* units = (Q == Q_FILLC) ? s.interp_c2 : (Q == Q_FILLC1 ? s.interp_c1 : s.interp_hg);
-    const size_t cap2 = 2 * (size_t)(s.max_blks + 1) * R;
-    const int nc = s.fillinfo[NQUEUES + Q], ni = s.fillinfo[2 * NQUEUES + Q];
-    const int nA = nc * F, nB = ni * (HG ? 18 : 1);
-    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nA + nB; u += gridDim.x * blockDim.x) {
-        if (u < nA) {
-            const int j = u % nc, f = u / nc;
-            const unsigned dst = (unsigned)__ldg(units + 2 * j), src = (unsigned)__ldg(units + 2 * j + 1);
-            double* A = HG ? (f ? s.Ag : s.Ah) : s.C;
-            if (HG) {
-                double v[9];
-#pragma unroll
-                for (int i = 0; i < 9; ++i) v[i] = __ldg(A + src + (size_t)i * G.aplane);
-#pragma unroll
-                for (int i = 0; i < 9; ++i) A[dst + (size_t)i * G.aplane] = v[i];
-            } else {
-                A[dst] = __ldg(A + src);
-            }
-            continue;
-        }
-        const int v = u - nA, j = HG ? v / 18 : v, fq = HG ? v % 18 : 0;
-        const unsigned dst = (unsigned)__ldg(units + cap2 - 2 - 2 * (size_t)j);
-        const int e = __ldg(units + cap2 - 1 - 2 * (size_t)j);
-        const int* pl = plans + (size_t)(e / R) * R * PLAN_INTS + e % R;
-        const int meta = __ldg(pl);
-        double* A = HG ? (fq >= 9 ? s.Ag : s.Ah) : s.C;
-        const size_t qo = (size_t)(fq % 9) * (HG ? G.aplane : 0);
-        double g[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) g[i] = __ldg(A + (unsigned)__ldg(pl + (1 + i) * R) + qo);
-        A[dst + qo] = plan_combine(meta, g);
-    }
-}
-
-// The coarse-to-fine ghost cells of block n (work position c) on the flat
-// path, into its staged copy and into memory. Sources: the coarser
-// neighbour's interior and its copies / fine-to-coarse cells, written by
-// k_fill_flat. T: shared C tile (index G.c(0,x,y)).
-template <int N>
-__device__ void c2f_cells_c(const DevState& s, const Geo<N>& G, int c, int n, int w, double* T) {
-    const int nx = G.nx, ny = G.ny;
-    const int R = (w == 2) ? ring2_len(nx, ny) : ring1_len(nx, ny);
-    const int* pl = ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)c * R * PLAN_INTS;
-    for (int t = threadIdx.x; t < R; t += blockDim.x) {
-        const int meta = __ldg(pl + t);
-        if (plan_kind(meta) != 3) continue;
-        int x, y;
-        if (w == 2)
-            ring2_xy(t, nx, ny, x, y);
-        else
-            ring1_xy(t, nx, ny, x, y);
-        double g[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)__ldg(pl + (1 + i) * R + t));
-        const double v = plan_combine(meta, g);
-        if (T) T[G.c(0, x, y)] = v;
-        s.C[G.c(n, x, y)] = v;
-    }
-}
-// The same for the h and g planes staged in As ([field][q][pool plane
-// layout]): one thread per (ghost cell, population), both fields.
-template <int N>
-__device__ void c2f_cells_hg(const DevState& s, const Geo<N>& G, int c, int n, double* As) {
-    const int nx = G.nx, ny = G.ny, RG = ring1_len(nx, ny), FP = 9 * G.aplane;
-    const int* pl = s.plan_hg + (size_t)c * RG * PLAN_INTS;
-    for (int idx = threadIdx.x; idx < 9 * RG; idx += blockDim.x) {
-        const int r = idx % RG, qq = idx / RG;
-        const int meta = __ldg(pl + r);
-        if (plan_kind(meta) != 3) continue;
-        int x, y;
-        ring1_xy(r, nx, ny, x, y);
-        unsigned o[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) o[i] = (unsigned)__ldg(pl + (1 + i) * RG + r) + qq * G.aplane;
-#pragma unroll
-        for (int f = 0; f < 2; ++f) {
-            double* A = f ? s.Ag : s.Ah;
-            double g[9];
-#pragma unroll
-            for (int i = 0; i < 9; ++i) g[i] = __ldg(A + o[i]);
-            const double v = plan_combine(meta, g);
-            As[f * FP + G.a(0, qq + 1, x, y)] = v;
-            A[G.a(n, qq + 1, x, y)] = v;
-        }
-    }
-}
-
-__host__ __device__ constexpr int fill_c_min_blocks(int consumer) {
-    return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) ? 2 : 3;
-}
-
-// Level-ordered C ghost fill of width w (Fill_Ghost_Cells_C.f90:2-416,
-// Fill_Ghost_Cells_C2.f90:2-416) and its consumer. Fill items: all leaves in
-// work order; leaves of levels outside [LevelMin, LevelMax] are not filled
-// (as the reference's DO L = LevelMin, LevelMax) but still get the consumer
-// work. A consumer item bulk-copies its block's C tile, ring included, into
-// one of two shared stages; the copy of the next item's tile starts while
-// the current one is consumed (at once if that block's fill is done, else
-// after the wait for it).
-template <int N, int CONSUMER>
-__global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
-    k_fill_c(DevState s, int w, int q) {
-    extern __shared__ __align__(128) unsigned char smraw[];
-    const Geo<N> G(s);
-    __shared__ NbInfo nbis[2];
-    __shared__ double red[32];
-    __shared__ int s_next;
-    const int t = threadIdx.x;
-    const int total = s.lvl_off[AMR_MAXLV];
-    // fast: k_fill_flat has filled every ring; the walls are left to the
-    // consumer items. Else the fill phase fills level by level, walls included.
-    const bool fast = flat_fill(s, q);
-    if (!fast)
-        fill_phase(
-            s, q, nbis, &s_next,
-            [&](int k, int n, const NbInfo& nbi) {
-                if (nbi.wait) {
-                    fill_c_ring<N>(s, G, k, n, w, 1);
-                    wait_coarse(s, q, nbi);
-                    fill_c_ring<N>(s, G, k, n, w, 2);
-                } else {
-                    fill_c_ring<N>(s, G, k, n, w, 0);
-                }
-            },
-            [&](int n, const NbInfo& nbi) { wall_c<N>(s, G, n, nbi, w); });
-    // item c's level (record word lev[0]) and walls (id[3], id[4] < 0)
-    auto rec_walls = [&](int c, int& L, bool& w3, bool& w4) {
-        const int* rec = s.nbinfo + (size_t)c * NBI_STRIDE;
-        L = __ldg(rec + 9);
-        w3 = __ldg(rec + 3) < 0;
-        w4 = __ldg(rec + 4) < 0;
-    };
-    if (CONSUMER == CONS_NONE) {  // flat path: coarse-to-fine cells and walls in memory
-        if (fast)
-            for (int c = blockIdx.x; c < total; c += gridDim.x) {
-                int L;
-                bool w3, w4;
-                rec_walls(c, L, w3, w4);
-                const int n = __ldg(s.lvl_leaf + c);
-                c2f_cells_c<N>(s, G, c, n, w, nullptr);
-                __syncthreads();
-                if (w3 || w4) wall_c_rows<N>(s, G, n, w, w3, w4, nullptr);
-                __syncthreads();
-            }
-        return;
-    }
-
-    constexpr bool collide = (CONSUMER == CONS_COLLIDE_READ || CONSUMER == CONS_COLLIDE_FUSED);
-    if (collide && blockIdx.x == 0 && t == 0)
-        atomicAdd(&s.cnt->updates, (unsigned long long)total * (unsigned long long)(G.nx * G.ny));
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw);  // [2]
-    double* tiles = reinterpret_cast<double*>(smraw + 128);
-    const unsigned tb = (unsigned)G.cplane * 8;
-    const int* flags = fill_flags(s, q);
-    // thread 0: copy item c's C tile into stage st once its fill is done;
-    // without `block` only if it is done already (returns whether it started)
-    auto start_tile = [&](int st, int c, bool block) {
-        const int nn = __ldg(s.lvl_leaf + c);
-        if (fast) {
-            // the ring was written by the previous launch
-        } else if (block) {
-            if (!spin_flag(flags + nn)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
-        } else if (ld_acquire_i(flags + nn) == 0) {
-            return false;
-        }
-        fence_proxy_async_all();
-        mbar_expect_tx(&bar[st], tb);
-        bulk_g2s(tiles + (size_t)st * G.cplane, s.C + (size_t)nn * G.cplane, tb, &bar[st]);
-        return true;
-    };
-    bool pend = false;  // thread 0: the next item's copy is still to start
-    if (t == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        const int c0 = (int)atomicAdd(&s.queue[2 * q + 1], 1u);
-        s_next = c0;
-        if (c0 < total) start_tile(0, c0, true);
-    }
-    __syncthreads();
-    int c = s_next;
-    unsigned phase = 0;  // bit st: parity of stage st's next completion
-    int st = 0;
-    while (c < total) {
-        unsigned cn = 0;
-        if (t == 0) cn = atomicAdd(&s.queue[2 * q + 1], 1u);
-        const int n = __ldg(s.lvl_leaf + c);
-        if (__syncthreads_or(mbar_wait(&bar[st], (phase >> st) & 1u) ? 0 : 1)) {
-            if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
-            mbar_wait(&bar[st], (phase >> st) & 1u);  // the copy must land before exit
-            break;
-        }
-        phase ^= 1u << st;
-        if (t == 0) {
-            s_next = (int)cn;
-            pend = ((int)cn < total) && !start_tile(st ^ 1, (int)cn, false);
-        }
-        double* T = tiles + (size_t)st * G.cplane;
-        if (fast) {  // coarse-to-fine cells, then Symmetric_C(2)_3/4, on the tile and in memory
-            int L;
-            bool w3, w4;
-            rec_walls(c, L, w3, w4);
-            c2f_cells_c<N>(s, G, c, n, w, T);
-            __syncthreads();
-            if (w3 || w4) {
-                wall_c_rows<N>(s, G, n, w, w3, w4, T);
-                __syncthreads();
-            }
-        }
-        if (CONSUMER == CONS_MACRO_G)
-            err_reduce(s, n, macro_g_block<N>(s, G, n, T), red);
-        else
-            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED>(s, G, n, T);
-        __syncthreads();
-        c = s_next;
-        st ^= 1;
-        if (t == 0 && pend) start_tile(st, c, true);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// h/g ghost ring of the item at work position k (block n) from its plans,
-// into memory (mode as fill_c_ring). A cell without a plan keeps its value in
-// memory. Copies take one thread per (ring cell, field) with the 9
-// populations' loads in flight together; interpolated cells one thread per
-// (ring cell, field, population) with the 9 stencil loads in flight together.
-template <int N>
-__device__ void fill_hg_ring(const DevState& s, const Geo<N>& G, int k, int n, int mode) {
-    const int nx = G.nx, ny = G.ny, RG = ring1_len(nx, ny);
-    const int* pl = s.plan_hg + (size_t)k * RG * PLAN_INTS;
-    if (mode != 2) {
-        for (int idx = threadIdx.x; idx < 2 * RG; idx += blockDim.x) {
-            const int r = idx % RG;
-            const int kind = plan_kind(__ldg(pl + r));
-            if (kind != 1 && kind != -1) continue;
-            int x, y;
-            ring1_xy(r, nx, ny, x, y);
-            if (kind < 0) {
-                set_error(s, 4 /*AMRLBM_ERR_LEVEL_JUMP*/, n);
-                continue;
-            }
-            double* A = (idx >= RG) ? s.Ag : s.Ah;
-            const double* src = A + (unsigned)__ldg(pl + RG + r);
-            double v[9];
-#pragma unroll
-            for (int qq = 0; qq < 9; ++qq) v[qq] = __ldg(src + (size_t)qq * G.aplane);
-#pragma unroll
-            for (int qq = 0; qq < 9; ++qq) A[G.a(n, qq + 1, x, y)] = v[qq];
-        }
-    }
-    for (int idx = threadIdx.x; idx < 18 * RG; idx += blockDim.x) {
-        const int r = idx % RG, fq = idx / RG;
-        const int meta = __ldg(pl + r);
-        const int kind = plan_kind(meta);
-        if (kind < 2 || !pass_takes(mode, kind)) continue;
-        int x, y;
-        ring1_xy(r, nx, ny, x, y);
-        const int qq = fq % 9;
-        double* A = (fq >= 9) ? s.Ag : s.Ah;
-        const size_t qo = (size_t)qq * G.aplane;
-        double g[9];
-        if (kind == 2) {
-#pragma unroll
-            for (int i = 0; i < 9; ++i) g[i] = __ldg(A + (unsigned)__ldg(pl + (1 + i) * RG + r) + qo);
-        } else {
-#pragma unroll
-            for (int i = 0; i < 9; ++i) g[i] = ldcg(A + (unsigned)__ldg(pl + (1 + i) * RG + r) + qo);
-        }
-        A[G.a(n, qq + 1, x, y)] = plan_combine(meta, g);
-    }
-}
-
 // Bounce_Back_3/4 (BC_Cell.f90:2-42): f(i,X,wall row) = f(opposite(i), Xn,
 // first row) on the walls of block n; after the ring fill and a barrier
 template <int N>
@@ -1025,7 +937,7 @@ __device__ void bounce_back(const DevState& s, const Geo<N>& G, int n, const NbI
 // wall rows are written, rows 1 and ny read.
 template <int N>
 __device__ void bounce_back_staged(const DevState& s, const Geo<N>& G, int n, bool w3, bool w4,
-                                   double* As) {
+                                   double* As, bool to_mem = true) {
     const int nx = G.nx, ny = G.ny, FP = 9 * G.aplane;
     for (int idx = threadIdx.x; idx < (nx + 2) * 36; idx += blockDim.x) {
         const int X = idx % (nx + 2), qf = (idx / (nx + 2)) % 18;
@@ -1040,7 +952,7 @@ __device__ void bounce_back_staged(const DevState& s, const Geo<N>& G, int n, bo
         }
         const double v = As[f * FP + G.a(0, J, Xn, Yi)];
         As[f * FP + G.a(0, i, X, Y)] = v;
-        (f ? s.Ag : s.Ah)[G.a(n, i, X, Y)] = v;
+        if (to_mem) (f ? s.Ag : s.Ah)[G.a(n, i, X, Y)] = v;
     }
 }
 
@@ -1081,12 +993,158 @@ __device__ void stream_block(const DevState& s, const Geo<N>& G, int n, const do
     }
 }
 
-// Level-ordered Fill_Ghost_Cells_hg (Fill_Ghost_Cells_hg.f90:2-477) with
-// Bounce_Back_3/4, then streaming and Macroscopic_Values_h_AMR of every leaf.
-// The ghost ring goes to memory; a streaming item waits for its own block's
-// fill, then bulk-copies the block's h and g planes into shared memory.
+__host__ __device__ constexpr int fill_c_min_blocks(int consumer) {
+    return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) ? 2 : 3;
+}
+
+// word offset of nf[] in a neighbour record
+constexpr int REC_NF = (int)(offsetof(NbInfo, nf) / sizeof(int));
+
+// C ghost fill of width w (Fill_Ghost_Cells_C.f90:2-416, Fill_Ghost_Cells_C2
+// .f90:2-416) with Symmetric_C(2)_3/4 and its consumer, one item per leaf in
+// work order. Without level order (fast_fill) an item bulk-copies its C tile
+// into one of two shared stages while the item before it is consumed, fills
+// its own ring on the tile and in memory, applies the walls and consumes.
+// With level order the fill phase fills every leaf first (leaves of levels
+// outside [LevelMin, LevelMax] are not filled, as the reference's DO L =
+// LevelMin, LevelMax, but still get the consumer work), and an item's tile
+// copy waits for its block's flag.
+// Shared memory: mbarriers (128 bytes), two C tiles, the foreign values.
+template <int N, int CONSUMER>
+__global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
+    k_fill_c(DevState s, int w, int q, int wr) {
+    extern __shared__ __align__(128) unsigned char smraw[];
+    const Geo<N> G(s);
+    __shared__ NbInfo nbis[2];
+    __shared__ double red[32];
+    __shared__ int s_next;
+    const int t = threadIdx.x;
+    const int total = s.lvl_off[AMR_MAXLV];
+    const int lmin = s.cnt->level_min;
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw);  // [2]
+    double* tiles = reinterpret_cast<double*>(smraw + 128);
+    double* Fs = tiles + 2 * (size_t)G.cplane;
+    const bool fast = fast_fill(s, q);
+    if (!fast)
+        fill_phase(
+            s, q, nbis, &s_next,
+            [&](int k, int n, const NbInfo& nbi) {
+                foreign_c<N>(s, k, w, nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
+                if (nbi.wait[q]) {
+                    fill_ring_c<N>(s, G, k, n, w, 1, Fs, nullptr);
+                    wait_coarse(s, q, nbi);
+                    fill_ring_c<N>(s, G, k, n, w, 2, Fs, nullptr);
+                } else {
+                    fill_ring_c<N>(s, G, k, n, w, 0, Fs, nullptr);
+                }
+            },
+            [&](int n, const NbInfo& nbi) { wall_c<N>(s, G, n, nbi, w); });
+    // item c's foreign cells and walls (id[3], id[4] < 0) from its record
+    auto rec = [&](int c, int& nf, bool& w3, bool& w4) {
+        const int* r = s.nbinfo + (size_t)c * NBI_STRIDE;
+        nf = __ldg(r + REC_NF + q);
+        w3 = __ldg(r + 3) < 0;
+        w4 = __ldg(r + 4) < 0;
+    };
+    if (CONSUMER == CONS_NONE) {  // Fill_Ghost_Cells_C(2) alone
+        if (fast)
+            for (int c = blockIdx.x; c < total; c += gridDim.x) {
+                int nf;
+                bool w3, w4;
+                rec(c, nf, w3, w4);
+                const int n = __ldg(s.lvl_leaf + c);
+                foreign_c<N>(s, c, w, nf, true, Fs);
+                fill_ring_c<N>(s, G, c, n, w, 0, Fs, nullptr);
+                __syncthreads();
+                if (w3 || w4) wall_c_rows<N>(s, G, n, w, w3, w4, nullptr);
+                __syncthreads();
+            }
+        return;
+    }
+
+    constexpr bool collide = (CONSUMER == CONS_COLLIDE_READ || CONSUMER == CONS_COLLIDE_FUSED);
+    if (collide && blockIdx.x == 0 && t == 0)
+        atomicAdd(&s.cnt->updates, (unsigned long long)total * (unsigned long long)(G.nx * G.ny));
+    const unsigned tb = (unsigned)G.cplane * 8;
+    const int* flags = fill_flags(s, q);
+    // thread 0: copy item c's C tile into stage st (with level order: once
+    // its fill is done; without `block` only if it is done already; returns
+    // whether the copy started)
+    auto start_tile = [&](int st, int c, bool block) {
+        const int nn = __ldg(s.lvl_leaf + c);
+        if (fast) {
+            // the interior was written by the previous launch
+        } else if (block) {
+            if (!spin_flag(flags + nn)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
+        } else if (ld_acquire_i(flags + nn) == 0) {
+            return false;
+        }
+        fence_proxy_async_all();
+        mbar_expect_tx(&bar[st], tb);
+        bulk_g2s(tiles + (size_t)st * G.cplane, s.C + (size_t)nn * G.cplane, tb, &bar[st]);
+        return true;
+    };
+    bool pend = false;  // thread 0: the next item's copy is still to start
+    if (t == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        const int c0 = (int)atomicAdd(&s.queue[2 * q + 1], 1u);
+        s_next = c0;
+        if (c0 < total) start_tile(0, c0, true);
+    }
+    __syncthreads();
+    int c = s_next;
+    unsigned phase = 0;  // bit st: parity of stage st's next completion
+    int st = 0;
+    while (c < total) {
+        unsigned cn = 0;
+        if (t == 0) cn = atomicAdd(&s.queue[2 * q + 1], 1u);
+        const int n = __ldg(s.lvl_leaf + c);
+        int nf = 0;
+        bool w3 = false, w4 = false;
+        if (fast) {
+            rec(c, nf, w3, w4);
+            foreign_c<N>(s, c, w, nf, true, Fs);  // while the tile lands
+        }
+        if (__syncthreads_or(mbar_wait(&bar[st], (phase >> st) & 1u) ? 0 : 1)) {
+            if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
+            mbar_wait(&bar[st], (phase >> st) & 1u);  // the copy must land before exit
+            break;
+        }
+        phase ^= 1u << st;
+        double* T = tiles + (size_t)st * G.cplane;
+        if (fast) {  // the ring, then Symmetric_C(2)_3/4, on the tile (and in memory if wr)
+            fill_ring_c<N>(s, G, c, n, w, 0, Fs, T, wr != 0);
+            __syncthreads();
+            if (w3 || w4) {
+                wall_c_rows<N>(s, G, n, w, w3, w4, T, wr != 0);
+                __syncthreads();
+            }
+        }
+        if (t == 0) {
+            s_next = (int)cn;
+            pend = ((int)cn < total) && !start_tile(st ^ 1, (int)cn, false);
+        }
+        if (CONSUMER == CONS_MACRO_G)
+            err_reduce(s, n, macro_g_block<N>(s, G, n, T), red);
+        else
+            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED>(s, G, n, T);
+        __syncthreads();
+        c = s_next;
+        st ^= 1;
+        if (t == 0 && pend) start_tile(st, c, true);
+    }
+}
+
+// Fill_Ghost_Cells_hg (Fill_Ghost_Cells_hg.f90:2-477) with Bounce_Back_3/4,
+// then streaming and Macroscopic_Values_h_AMR, one item per leaf in work
+// order. Each item bulk-copies its block's h and g planes into shared memory;
+// without level order (fast_fill) it fills its own ring there and in memory
+// and applies the walls; with level order the fill phase fills every leaf
+// first and the copy waits for the block's flag.
+// Shared memory: mbarrier (128 bytes), h and g planes, the foreign values.
 template <int N>
-__global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s) {
+__global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const Geo<N> G(s);
     __shared__ NbInfo nbis[2];
@@ -1094,25 +1152,26 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s) {
     const int q = Q_FILLHG;
     const int t = threadIdx.x;
     const int total = s.lvl_off[AMR_MAXLV];
-    // fast: k_fill_flat has filled every ring; bounce-back is left to the
-    // streaming items. Else the fill phase fills level by level, walls included.
-    const bool fast = flat_fill(s, q);
+    const int lmin = s.cnt->level_min;
+    const int FP = 9 * G.aplane;
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw);
+    double* As = reinterpret_cast<double*>(smraw + 128);  // [h|g][q][pool plane layout]
+    double* Fs = As + 2 * (size_t)FP;
+    const bool fast = fast_fill(s, q);
     if (!fast)
         fill_phase(
             s, q, nbis, &s_next,
             [&](int k, int n, const NbInfo& nbi) {
-                if (nbi.wait) {
-                    fill_hg_ring<N>(s, G, k, n, 1);
+                foreign_hg<N>(s, G, k, nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
+                if (nbi.wait[q]) {
+                    fill_ring_hg<N>(s, G, k, n, 1, Fs, nullptr);
                     wait_coarse(s, q, nbi);
-                    fill_hg_ring<N>(s, G, k, n, 2);
+                    fill_ring_hg<N>(s, G, k, n, 2, Fs, nullptr);
                 } else {
-                    fill_hg_ring<N>(s, G, k, n, 0);
+                    fill_ring_hg<N>(s, G, k, n, 0, Fs, nullptr);
                 }
             },
             [&](int n, const NbInfo& nbi) { bounce_back<N>(s, G, n, nbi); });
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw);
-    double* As = reinterpret_cast<double*>(smraw + 128);  // [h|g][q][pool plane layout]
-    const int FP = 9 * G.aplane;
     const unsigned fb = (unsigned)FP * 8;
     const int* flags = fill_flags(s, q);
     if (t == 0) {
@@ -1134,19 +1193,24 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s) {
             bulk_g2s(As + FP, s.Ag + (size_t)n * FP, fb, bar);
             s_next = (int)cn;
         }
+        bool w3 = false, w4 = false;
+        if (fast) {
+            const int* r = s.nbinfo + (size_t)c * NBI_STRIDE;
+            w3 = __ldg(r + 3) < 0;
+            w4 = __ldg(r + 4) < 0;
+            foreign_hg<N>(s, G, c, __ldg(r + REC_NF + q), true, Fs);  // while the planes land
+        }
         if (__syncthreads_or(mbar_wait(bar, phase) ? 0 : 1)) {
             if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
             mbar_wait(bar, phase);  // the copies must land before exit
             break;
         }
         phase ^= 1u;
-        if (fast) {  // coarse-to-fine cells, then Bounce_Back_3/4, on the staged planes and in memory
-            const int* rec = s.nbinfo + (size_t)c * NBI_STRIDE;
-            const bool w3 = __ldg(rec + 3) < 0, w4 = __ldg(rec + 4) < 0;
-            c2f_cells_hg<N>(s, G, c, n, As);
+        if (fast) {  // the ring, then Bounce_Back_3/4, on the staged planes (and in memory if wr)
+            fill_ring_hg<N>(s, G, c, n, 0, Fs, As, wr != 0);
             __syncthreads();
             if (w3 || w4) {
-                bounce_back_staged<N>(s, G, n, w3, w4, As);
+                bounce_back_staged<N>(s, G, n, w3, w4, As, wr != 0);
                 __syncthreads();
             }
         }
@@ -1292,25 +1356,28 @@ int queue_grid(K kernel, int nt, size_t smem, const LaunchCfg& lc) {
     return lc.num_sms * occ;
 }
 
-// shared memory of a C-fill launch: mbarriers, two C tiles
-size_t fill_c_smem(const DevState& s) { return 128 + 2 * sizeof(double) * (size_t)s.cplane; }
+// shared memory of a C-fill launch: mbarriers, two C tiles, foreign values
+size_t fill_c_smem(const DevState& s) {
+    return 128 + sizeof(double) * (2 * (size_t)s.cplane + (size_t)s.fmax);
+}
 
 template <int N, int CONS>
-void fill_c_launch(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width, int q) {
+void fill_c_launch(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width, int q,
+                   int wr) {
     const size_t sm = fill_c_smem(s);
     const int nt = block_threads(s);
     smem_optin(k_fill_c<N, CONS>, sm);
-    k_fill_c<N, CONS><<<queue_grid(k_fill_c<N, CONS>, nt, sm, lc), nt, sm, st>>>(s, width, q);
+    k_fill_c<N, CONS><<<queue_grid(k_fill_c<N, CONS>, nt, sm, lc), nt, sm, st>>>(s, width, q, wr);
 }
 
 template <int N>
 void fill_c_dispatch(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width,
-                     int consumer, int q) {
+                     int consumer, int q, int wr) {
     switch (consumer) {
-        case CONS_NONE: fill_c_launch<N, CONS_NONE>(s, lc, st, width, q); break;
-        case CONS_COLLIDE_READ: fill_c_launch<N, CONS_COLLIDE_READ>(s, lc, st, width, q); break;
-        case CONS_COLLIDE_FUSED: fill_c_launch<N, CONS_COLLIDE_FUSED>(s, lc, st, width, q); break;
-        default: fill_c_launch<N, CONS_MACRO_G>(s, lc, st, width, q); break;
+        case CONS_NONE: fill_c_launch<N, CONS_NONE>(s, lc, st, width, q, wr); break;
+        case CONS_COLLIDE_READ: fill_c_launch<N, CONS_COLLIDE_READ>(s, lc, st, width, q, wr); break;
+        case CONS_COLLIDE_FUSED: fill_c_launch<N, CONS_COLLIDE_FUSED>(s, lc, st, width, q, wr); break;
+        default: fill_c_launch<N, CONS_MACRO_G>(s, lc, st, width, q, wr); break;
     }
 }
 
@@ -1325,46 +1392,35 @@ void fill_c_dispatch(const DevState& s, const LaunchCfg& lc, cudaStream_t st, in
 
 // ---------------------------------------------------------------------------
 void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width,
-                   int consumer) {
+                   int consumer, int write_ring) {
     const int q = (width == 2) ? Q_FILLC : Q_FILLC1;
     cudaMemsetAsync(s.queue + 2 * q, 0, 2 * sizeof(unsigned), st);
     cudaMemsetAsync(s.ring_done + (size_t)q * (s.max_blks + 1), 0,
                     sizeof(int) * (size_t)(s.max_blks + 1), st);
-#define F_(N)                                                      \
-    if (width == 2)                                                \
-        k_fill_flat<N, Q_FILLC><<<lc.num_sms * 8, 256, 0, st>>>(s);  \
-    else                                                           \
-        k_fill_flat<N, Q_FILLC1><<<lc.num_sms * 8, 256, 0, st>>>(s)
-    DISPATCH(s, F_);
-#undef F_
-    count_launches(1);
-#define C_(N) fill_c_dispatch<N>(s, lc, st, width, consumer, q)
+#define C_(N) fill_c_dispatch<N>(s, lc, st, width, consumer, q, write_ring)
     DISPATCH(s, C_);
 #undef C_
     count_launches(1);
 }
 
-void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
+void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int write_ring) {
     cudaMemsetAsync(s.queue + 2 * Q_FILLHG, 0, 2 * sizeof(unsigned), st);
     cudaMemsetAsync(s.ring_done + (size_t)Q_FILLHG * (s.max_blks + 1), 0,
                     sizeof(int) * (size_t)(s.max_blks + 1), st);
-#define F_(N) k_fill_flat<N, Q_FILLHG><<<lc.num_sms * 8, 256, 0, st>>>(s)
-    DISPATCH(s, F_);
-#undef F_
-    count_launches(1);
     const int nt = block_threads(s);
-    const size_t sm = 128 + 18 * sizeof(double) * (size_t)s.aplane;  // mbarrier, h and g planes
+    // mbarrier, h and g planes, foreign values
+    const size_t sm = 128 + 18 * sizeof(double) * ((size_t)s.aplane + (size_t)s.fmax);
 #define C_(N)                                                                            \
     smem_optin(k_fill_hg_stream<N>, sm);                                                 \
-    k_fill_hg_stream<N><<<queue_grid(k_fill_hg_stream<N>, nt, sm, lc), nt, sm, st>>>(s)
+    k_fill_hg_stream<N><<<queue_grid(k_fill_hg_stream<N>, nt, sm, lc), nt, sm, st>>>(s, write_ring)
     DISPATCH(s, C_);
 #undef C_
     count_launches(1);
 }
 
 void launch_build_plans(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
-    cudaMemsetAsync(s.fillinfo, 0, 3 * NQUEUES * sizeof(int), st);
-#define C_(N) k_build_plans<N><<<lc.grid_leaves, 128, 0, st>>>(s)
+    cudaMemsetAsync(s.fillinfo, 0, NQUEUES * sizeof(int), st);
+#define C_(N) k_build_plans<N><<<lc.grid_leaves, 128, 9 * sizeof(int) * ring1_len(s.nx, s.ny), st>>>(s)
     DISPATCH(s, C_);
 #undef C_
     count_launches(1);
@@ -1416,3 +1472,4 @@ int selftest_division(unsigned long long n, unsigned long long seed, double divi
     cudaFree(d);
     return e == cudaSuccess ? 0 : 2;
 }
+
