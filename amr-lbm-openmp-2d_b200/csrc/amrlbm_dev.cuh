@@ -45,7 +45,7 @@ enum { Q_FILLC = 0, Q_FILLHG = 1, Q_FILLC1 = 2, NQUEUES = 3 };
 // per-leaf records of the level-ordered kernels, indexed by work-order
 // position: neighbour record (NBI_STRIDE ints) and one fill plan per ghost
 // cell (PLAN_INTS ints: kind/weights word + 9 source offsets)
-enum { NBI_STRIDE = 48, PLAN_INTS = 10 };
+enum { NBI_STRIDE = 64, PLAN_INTS = 10 };
 
 // ---------------------------------------------------------------------------
 // The block pool. Block ids are 1..max_blks (slot 0 unused).

@@ -56,6 +56,7 @@ struct NbInfo {
     int bi, bj;
     int wait[NQUEUES];
     int nf[NQUEUES];
+    int na[NQUEUES], nb[NQUEUES];  // plan entries of kinds 1/-1 and 2/3 (stored first)
 };
 constexpr int NBI_INTS = (int)(sizeof(NbInfo) / sizeof(int));
 static_assert(NBI_INTS <= NBI_STRIDE, "NbInfo record");
@@ -158,12 +159,13 @@ __device__ __forceinline__ void ghost_plan(const NbInfo& nbi, int nx, int ny, in
 }
 
 // Packed plan of one ghost cell, stored plane by plane: plane 0 holds the
-// meta word (bits 0-2 kind+1, bit 3 Jx, bit 4 Jy: the stencil weights are
+// meta word (bits 0-2 kind+1, bit 3 Jx, bit 4 Jy, bits 8- the cell's ring
+// index; the stencil weights are
 // ax = 3-4Jx (fine) or 5-8Jx (coarse), cx = 2-ax, the same along y), planes
 // 1..9 the source offsets (in doubles, into the C pool or the first plane of
 // the A pool). Plane i of entry t of a ring of R entries is base[i*R + t].
-__device__ __forceinline__ void plan_store(int* base, int R, int t, const GPlan& P) {
-    int meta = (P.kind + 1) & 7;
+__device__ __forceinline__ void plan_store(int* base, int R, int t, const GPlan& P, int ring = 0) {
+    int meta = ((P.kind + 1) & 7) | (ring << 8);
     if (P.kind == 2) meta |= ((P.ax == -1) ? 8 : 0) | ((P.ay == -1) ? 16 : 0);
     if (P.kind == 3) meta |= ((P.ax == -3) ? 8 : 0) | ((P.ay == -3) ? 16 : 0);
     base[t] = meta;
@@ -280,6 +282,7 @@ __global__ void k_build_plans(DevState s) {
     __shared__ NbInfo nbi;
     __shared__ NbInfo cnb[9];     // coarser neighbours' records
     __shared__ int nfs;
+    __shared__ int cls_n[2][3], cls_f[2][3];  // [C2 | ring-1 plans][class]: count, fill
     const int nx = G.nx, ny = G.ny, R2 = ring2_len(nx, ny), R1 = ring1_len(nx, ny);
     const int total = s.lvl_off[AMR_MAXLV];
     const int t = threadIdx.x, fmax = s.fmax;
@@ -288,6 +291,10 @@ __global__ void k_build_plans(DevState s) {
         if (t == 0) {
             load_nbinfo(s, n, nbi);
             nfs = 0;
+        }
+        if (t < 6) {
+            cls_n[t / 3][t % 3] = 0;
+            cls_f[t / 3][t % 3] = 0;
         }
         for (int i = t; i < 9 * R1; i += blockDim.x) tab[i] = -1;
         __syncthreads();
@@ -326,6 +333,11 @@ __global__ void k_build_plans(DevState s) {
                            return 0;
                        },
                        P);
+            // entries are stored by class: copies and level jumps, interpolated
+            // cells, cells without a plan
+            const int cls = (P.kind == 1 || P.kind < 0) ? 0 : (P.kind >= 2 ? 1 : 2);
+            atomicAdd(&cls_n[0][cls], 1);
+            if (r1) atomicAdd(&cls_n[1][cls], 1);
             if (P.kind < 0) {  // the level jump is reported by the level-ordered fills
                 atomicOr(&s.fillinfo[Q_FILLC], 1);
                 if (r1) {
@@ -367,6 +379,9 @@ __global__ void k_build_plans(DevState s) {
         __syncthreads();
         if (t < NQUEUES) {
             nbi.nf[t] = nfs;
+            const int pt = (t == Q_FILLC) ? 0 : 1;
+            nbi.na[t] = cls_n[pt][0];
+            nbi.nb[t] = cls_n[pt][1];
             if (nbi.wait[t]) atomicOr(&s.fillinfo[t], 1);
         }
         // 3: the plans, foreign cells by slot
@@ -391,12 +406,17 @@ __global__ void k_build_plans(DevState s) {
                            return w;
                        },
                        P);
-            plan_store(s.plan_c2 + (size_t)k * R2 * PLAN_INTS, R2, i, P);
+            const int cls = (P.kind == 1 || P.kind < 0) ? 0 : (P.kind >= 2 ? 1 : 2);
+            auto slot = [&](int pt) {
+                return (cls > 0 ? cls_n[pt][0] : 0) + (cls > 1 ? cls_n[pt][1] : 0) +
+                       atomicAdd(&cls_f[pt][cls], 1);
+            };
+            plan_store(s.plan_c2 + (size_t)k * R2 * PLAN_INTS, R2, slot(0), P, i);
             if (x >= 0 && x <= nx + 1 && y >= 0 && y <= ny + 1) {
-                const int i1 = ring1_index(x, y, nx, ny);
-                plan_store(s.plan_c1 + (size_t)k * R1 * PLAN_INTS, R1, i1, P);
+                const int i1 = ring1_index(x, y, nx, ny), e1 = slot(1);
+                plan_store(s.plan_c1 + (size_t)k * R1 * PLAN_INTS, R1, e1, P, i1);
                 for (int m = 0; m < 9; ++m) P.src[m] = aoff[m];
-                plan_store(s.plan_hg + (size_t)k * R1 * PLAN_INTS, R1, i1, P);
+                plan_store(s.plan_hg + (size_t)k * R1 * PLAN_INTS, R1, e1, P, i1);
             }
         }
         __syncthreads();
@@ -583,38 +603,40 @@ __device__ __forceinline__ bool pass_takes(int mode, int kind) {
 // C ghost ring of width w of item k (block n) from its plans, into memory
 // (unless to_mem is false) and, if T is given, into the block's shared C tile
 // (index G.c(0,x,y)). Kind 1 and 2 sources are interiors no launch of this
-// fill writes.
+// fill writes. The plan entries are stored by class (copies, interpolated
+// cells, cells without a plan): pass 0 visits only the first na + nb.
 template <int N>
 __device__ void fill_ring_c(const DevState& s, const Geo<N>& G, int k, int n, int w, int mode,
-                            const double* Fs, double* T, bool to_mem = true) {
+                            int nab, const double* Fs, double* T, bool to_mem = true) {
     const int nx = G.nx, ny = G.ny;
     const int R = (w == 2) ? ring2_len(nx, ny) : ring1_len(nx, ny);
     const int* pl = ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)k * R * PLAN_INTS;
-    for (int t = threadIdx.x; t < R; t += blockDim.x) {
-        const int meta = __ldg(pl + t);
+    const int lim = (mode == 0) ? nab : R;
+    for (int e = threadIdx.x; e < lim; e += blockDim.x) {
+        const int meta = __ldg(pl + e);
         const int kind = plan_kind(meta);
         if (kind == 0 || !pass_takes(mode, kind)) continue;
         int x, y;
         if (w == 2)
-            ring2_xy(t, nx, ny, x, y);
+            ring2_xy(meta >> 8, nx, ny, x, y);
         else
-            ring1_xy(t, nx, ny, x, y);
+            ring1_xy(meta >> 8, nx, ny, x, y);
         if (kind < 0) {
             set_error(s, 4 /*AMRLBM_ERR_LEVEL_JUMP*/, n);
             continue;
         }
         double v;
         if (kind == 1) {
-            v = __ldg(s.C + (unsigned)__ldg(pl + R + t));
+            v = __ldg(s.C + (unsigned)__ldg(pl + R + e));
         } else {
             double g[9];
             if (kind == 2) {
 #pragma unroll
-                for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)__ldg(pl + (1 + i) * R + t));
+                for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)__ldg(pl + (1 + i) * R + e));
             } else {
 #pragma unroll
                 for (int i = 0; i < 9; ++i)
-                    g[i] = c2f_source((unsigned)__ldg(pl + (1 + i) * R + t), Fs, s.C, 0);
+                    g[i] = c2f_source((unsigned)__ldg(pl + (1 + i) * R + e), Fs, s.C, 0);
             }
             v = plan_combine(meta, g);
         }
@@ -623,66 +645,88 @@ __device__ void fill_ring_c(const DevState& s, const Geo<N>& G, int k, int n, in
     }
 }
 
+// One copied h/g ghost cell (plan entry e, field f): the 9 populations'
+// loads in flight together.
+template <int N>
+__device__ __forceinline__ void hg_copy(const DevState& s, const Geo<N>& G, const int* pl, int RG,
+                                        int e, int f, int n, double* As, bool to_mem) {
+    const int meta = __ldg(pl + e);
+    int x, y;
+    ring1_xy(meta >> 8, G.nx, G.ny, x, y);
+    if (plan_kind(meta) < 0) {
+        set_error(s, 4 /*AMRLBM_ERR_LEVEL_JUMP*/, n);
+        return;
+    }
+    double* A = f ? s.Ag : s.Ah;
+    const double* src = A + (unsigned)__ldg(pl + RG + e);
+    double v[9];
+#pragma unroll
+    for (int qq = 0; qq < 9; ++qq) v[qq] = __ldg(src + (size_t)qq * G.aplane);
+#pragma unroll
+    for (int qq = 0; qq < 9; ++qq) {
+        if (to_mem) A[G.a(n, qq + 1, x, y)] = v[qq];
+        if (As) As[f * 9 * G.aplane + G.a(0, qq + 1, x, y)] = v[qq];
+    }
+}
+// One interpolated h/g ghost cell (plan entry e, population qq), both fields.
+template <int N>
+__device__ __forceinline__ void hg_interp(const DevState& s, const Geo<N>& G, const int* pl, int RG,
+                                          int e, int qq, int n, const double* Fs, double* As,
+                                          bool to_mem) {
+    const int meta = __ldg(pl + e);
+    const int kind = plan_kind(meta);
+    int x, y;
+    ring1_xy(meta >> 8, G.nx, G.ny, x, y);
+    const size_t qo = (size_t)qq * G.aplane;
+    unsigned wd[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) wd[i] = (unsigned)__ldg(pl + (1 + i) * RG + e);
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        double* A = f ? s.Ag : s.Ah;
+        double g[9];
+        if (kind == 2) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) g[i] = __ldg(A + wd[i] + qo);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) g[i] = c2f_source(wd[i], Fs + (f * 9 + qq) * s.fmax, A, qo);
+        }
+        const double v = plan_combine(meta, g);
+        if (to_mem) A[G.a(n, qq + 1, x, y)] = v;
+        if (As) As[f * 9 * G.aplane + G.a(0, qq + 1, x, y)] = v;
+    }
+}
+
 // h/g ghost ring of item k (block n) from its plans, into memory (unless
 // to_mem is false) and, if As is given, into the block's staged planes
-// ([field][q][pool plane layout]).
-// A cell without a plan keeps its value in memory. Copies take one thread per
-// (ghost cell, field) with the 9 populations' loads in flight together;
-// interpolated cells one thread per (ghost cell, population), both fields.
+// ([field][q][pool plane layout]). A cell without a plan keeps its value in
+// memory. Pass 0 runs its na copies (per field) and nb interpolated cells
+// (per population) as one set of units; passes 1 and 2 filter all entries.
 template <int N>
-__device__ void fill_ring_hg(const DevState& s, const Geo<N>& G, int k, int n, int mode,
-                             const double* Fs, double* As, bool to_mem = true) {
-    const int nx = G.nx, ny = G.ny, RG = ring1_len(nx, ny), FP = 9 * G.aplane;
+__device__ void fill_ring_hg(const DevState& s, const Geo<N>& G, int k, int n, int mode, int na,
+                             int nb, const double* Fs, double* As, bool to_mem = true) {
+    const int RG = ring1_len(G.nx, G.ny);
     const int* pl = s.plan_hg + (size_t)k * RG * PLAN_INTS;
-    if (mode != 2) {
-        for (int idx = threadIdx.x; idx < 2 * RG; idx += blockDim.x) {
-            const int r = idx % RG, f = idx / RG;
-            const int kind = plan_kind(__ldg(pl + r));
-            if (kind != 1 && kind != -1) continue;
-            int x, y;
-            ring1_xy(r, nx, ny, x, y);
-            if (kind < 0) {
-                set_error(s, 4 /*AMRLBM_ERR_LEVEL_JUMP*/, n);
-                continue;
-            }
-            double* A = f ? s.Ag : s.Ah;
-            const double* src = A + (unsigned)__ldg(pl + RG + r);
-            double v[9];
-#pragma unroll
-            for (int qq = 0; qq < 9; ++qq) v[qq] = __ldg(src + (size_t)qq * G.aplane);
-#pragma unroll
-            for (int qq = 0; qq < 9; ++qq) {
-                if (to_mem) A[G.a(n, qq + 1, x, y)] = v[qq];
-                if (As) As[f * FP + G.a(0, qq + 1, x, y)] = v[qq];
-            }
+    if (mode == 0) {
+        for (int u = threadIdx.x; u < 2 * na + 9 * nb; u += blockDim.x) {
+            if (u < 2 * na)
+                hg_copy<N>(s, G, pl, RG, u % na, u / na, n, As, to_mem);
+            else
+                hg_interp<N>(s, G, pl, RG, na + (u - 2 * na) % nb, (u - 2 * na) / nb, n, Fs, As,
+                             to_mem);
         }
+        return;
     }
-    for (int idx = threadIdx.x; idx < 9 * RG; idx += blockDim.x) {
-        const int r = idx % RG, qq = idx / RG;
-        const int meta = __ldg(pl + r);
-        const int kind = plan_kind(meta);
-        if (kind < 2 || !pass_takes(mode, kind)) continue;
-        int x, y;
-        ring1_xy(r, nx, ny, x, y);
-        const size_t qo = (size_t)qq * G.aplane;
-        unsigned wd[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) wd[i] = (unsigned)__ldg(pl + (1 + i) * RG + r);
-#pragma unroll
-        for (int f = 0; f < 2; ++f) {
-            double* A = f ? s.Ag : s.Ah;
-            double g[9];
-            if (kind == 2) {
-#pragma unroll
-                for (int i = 0; i < 9; ++i) g[i] = __ldg(A + wd[i] + qo);
-            } else {
-#pragma unroll
-                for (int i = 0; i < 9; ++i) g[i] = c2f_source(wd[i], Fs + (f * 9 + qq) * s.fmax, A, qo);
-            }
-            const double v = plan_combine(meta, g);
-            if (to_mem) A[G.a(n, qq + 1, x, y)] = v;
-            if (As) As[f * FP + G.a(0, qq + 1, x, y)] = v;
+    if (mode == 1)
+        for (int u = threadIdx.x; u < 2 * RG; u += blockDim.x) {
+            const int kind = plan_kind(__ldg(pl + u % RG));
+            if (kind == 1 || kind == -1) hg_copy<N>(s, G, pl, RG, u % RG, u / RG, n, As, to_mem);
         }
+    for (int u = threadIdx.x; u < 9 * RG; u += blockDim.x) {
+        const int kind = plan_kind(__ldg(pl + u % RG));
+        if (kind >= 2 && pass_takes(mode, kind))
+            hg_interp<N>(s, G, pl, RG, u % RG, u / RG, n, Fs, As, to_mem);
     }
 }
 
@@ -997,18 +1041,47 @@ __host__ __device__ constexpr int fill_c_min_blocks(int consumer) {
     return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) ? 2 : 3;
 }
 
-// word offset of nf[] in a neighbour record
+// word offsets in a neighbour record
 constexpr int REC_NF = (int)(offsetof(NbInfo, nf) / sizeof(int));
+constexpr int REC_NA = (int)(offsetof(NbInfo, na) / sizeof(int));
+constexpr int REC_NB = (int)(offsetof(NbInfo, nb) / sizeof(int));
+
+// what an item of fill q needs from its record: block, foreign cells, plan
+// entry classes, walls (id[3], id[4] < 0)
+struct ItemRec {
+    int n, nf, na, nb;
+    bool w3, w4;
+};
+// the same words staged in shared memory by threads 0..5 (ItemRec from there)
+__device__ __forceinline__ void item_rec_stage(const DevState& s, int c, int q, int* dst) {
+    const int t = threadIdx.x;
+    if (t < 6) {
+        // n, nf, na, nb, id[3] (bottom), id[4] (top)
+        const int off = t == 0 ? 0 : t == 1 ? REC_NF + q : t == 2 ? REC_NA + q : t == 3 ? REC_NB + q : t - 1;
+        dst[t] = __ldg(s.nbinfo + (size_t)c * NBI_STRIDE + off);
+    }
+}
+__device__ __forceinline__ ItemRec item_rec_of(const int* w) {
+    ItemRec o;
+    o.n = w[0];
+    o.nf = w[1];
+    o.na = w[2];
+    o.nb = w[3];
+    o.w3 = w[4] < 0;
+    o.w4 = w[5] < 0;
+    return o;
+}
 
 // C ghost fill of width w (Fill_Ghost_Cells_C.f90:2-416, Fill_Ghost_Cells_C2
-// .f90:2-416) with Symmetric_C(2)_3/4 and its consumer, one item per leaf in
-// work order. Without level order (fast_fill) an item bulk-copies its C tile
-// into one of two shared stages while the item before it is consumed, fills
-// its own ring on the tile and in memory, applies the walls and consumes.
-// With level order the fill phase fills every leaf first (leaves of levels
-// outside [LevelMin, LevelMax] are not filled, as the reference's DO L =
-// LevelMin, LevelMax, but still get the consumer work), and an item's tile
-// copy waits for its block's flag.
+// .f90:2-416) with Symmetric_C(2)_3/4 and its consumer, one item per leaf.
+// Without level order (fast_fill) the items have no dependences: CTA b takes
+// items b, b + gridDim.x, ..., bulk-copies the next item's C tile into the
+// other of two shared stages while it consumes the current one, and fills
+// each item's ring on its tile (and in memory if wr), applies the walls and
+// consumes. With level order the fill phase fills every leaf first (leaves of
+// levels outside [LevelMin, LevelMax] are not filled, as the reference's DO
+// L = LevelMin, LevelMax, but still get the consumer work), and consumer
+// items are claimed from a queue, their tile copy waiting for the block's flag.
 // Shared memory: mbarriers (128 bytes), two C tiles, the foreign values.
 template <int N, int CONSUMER>
 __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
@@ -1020,52 +1093,56 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     __shared__ int s_next;
     const int t = threadIdx.x;
     const int total = s.lvl_off[AMR_MAXLV];
-    const int lmin = s.cnt->level_min;
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw);  // [2]
     double* tiles = reinterpret_cast<double*>(smraw + 128);
     double* Fs = tiles + 2 * (size_t)G.cplane;
     const bool fast = fast_fill(s, q);
+    constexpr bool collide = (CONSUMER == CONS_COLLIDE_READ || CONSUMER == CONS_COLLIDE_FUSED);
+    if (collide && blockIdx.x == 0 && t == 0)
+        atomicAdd(&s.cnt->updates, (unsigned long long)total * (unsigned long long)(G.nx * G.ny));
+    auto consume = [&](int n, const double* T) {
+        if (CONSUMER == CONS_MACRO_G)
+            err_reduce(s, n, macro_g_block<N>(s, G, n, T), red);
+        else if (CONSUMER != CONS_NONE)
+            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED>(s, G, n, T);
+    };
+    const unsigned tb = (unsigned)G.cplane * 8;
+    auto copy_tile = [&](int st, int nn) {  // thread 0
+        fence_proxy_async_all();
+        mbar_expect_tx(&bar[st], tb);
+        bulk_g2s(tiles + (size_t)st * G.cplane, s.C + (size_t)nn * G.cplane, tb, &bar[st]);
+    };
+
+    const int lmin = s.cnt->level_min;
     if (!fast)
         fill_phase(
             s, q, nbis, &s_next,
             [&](int k, int n, const NbInfo& nbi) {
                 foreign_c<N>(s, k, w, nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
                 if (nbi.wait[q]) {
-                    fill_ring_c<N>(s, G, k, n, w, 1, Fs, nullptr);
+                    fill_ring_c<N>(s, G, k, n, w, 1, 0, Fs, nullptr);
                     wait_coarse(s, q, nbi);
-                    fill_ring_c<N>(s, G, k, n, w, 2, Fs, nullptr);
+                    fill_ring_c<N>(s, G, k, n, w, 2, 0, Fs, nullptr);
                 } else {
-                    fill_ring_c<N>(s, G, k, n, w, 0, Fs, nullptr);
+                    fill_ring_c<N>(s, G, k, n, w, 0, nbi.na[q] + nbi.nb[q], Fs, nullptr);
                 }
             },
             [&](int n, const NbInfo& nbi) { wall_c<N>(s, G, n, nbi, w); });
-    // item c's foreign cells and walls (id[3], id[4] < 0) from its record
-    auto rec = [&](int c, int& nf, bool& w3, bool& w4) {
-        const int* r = s.nbinfo + (size_t)c * NBI_STRIDE;
-        nf = __ldg(r + REC_NF + q);
-        w3 = __ldg(r + 3) < 0;
-        w4 = __ldg(r + 4) < 0;
-    };
-    if (CONSUMER == CONS_NONE) {  // Fill_Ghost_Cells_C(2) alone
+    __shared__ int srec[2][6];  // without level order: records of the current and the next item
+    if (CONSUMER == CONS_NONE) {  // Fill_Ghost_Cells_C(2) alone: without level order, the rings in memory
         if (fast)
             for (int c = blockIdx.x; c < total; c += gridDim.x) {
-                int nf;
-                bool w3, w4;
-                rec(c, nf, w3, w4);
-                const int n = __ldg(s.lvl_leaf + c);
-                foreign_c<N>(s, c, w, nf, true, Fs);
-                fill_ring_c<N>(s, G, c, n, w, 0, Fs, nullptr);
+                item_rec_stage(s, c, q, srec[0]);
                 __syncthreads();
-                if (w3 || w4) wall_c_rows<N>(s, G, n, w, w3, w4, nullptr);
+                const ItemRec r = item_rec_of(srec[0]);
+                foreign_c<N>(s, c, w, r.nf, true, Fs);
+                fill_ring_c<N>(s, G, c, r.n, w, 0, r.na + r.nb, Fs, nullptr);
+                __syncthreads();
+                if (r.w3 || r.w4) wall_c_rows<N>(s, G, r.n, w, r.w3, r.w4, nullptr);
                 __syncthreads();
             }
         return;
     }
-
-    constexpr bool collide = (CONSUMER == CONS_COLLIDE_READ || CONSUMER == CONS_COLLIDE_FUSED);
-    if (collide && blockIdx.x == 0 && t == 0)
-        atomicAdd(&s.cnt->updates, (unsigned long long)total * (unsigned long long)(G.nx * G.ny));
-    const unsigned tb = (unsigned)G.cplane * 8;
     const int* flags = fill_flags(s, q);
     // thread 0: copy item c's C tile into stage st (with level order: once
     // its fill is done; without `block` only if it is done already; returns
@@ -1079,32 +1156,36 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         } else if (ld_acquire_i(flags + nn) == 0) {
             return false;
         }
-        fence_proxy_async_all();
-        mbar_expect_tx(&bar[st], tb);
-        bulk_g2s(tiles + (size_t)st * G.cplane, s.C + (size_t)nn * G.cplane, tb, &bar[st]);
+        copy_tile(st, nn);
         return true;
     };
     bool pend = false;  // thread 0: the next item's copy is still to start
     if (t == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
-        const int c0 = (int)atomicAdd(&s.queue[2 * q + 1], 1u);
+        const int c0 = fast ? (int)blockIdx.x : (int)atomicAdd(&s.queue[2 * q + 1], 1u);
         s_next = c0;
         if (c0 < total) start_tile(0, c0, true);
     }
+    if (fast && (int)blockIdx.x < total) item_rec_stage(s, blockIdx.x, q, srec[0]);
     __syncthreads();
     int c = s_next;
     unsigned phase = 0;  // bit st: parity of stage st's next completion
     int st = 0;
     while (c < total) {
-        unsigned cn = 0;
-        if (t == 0) cn = atomicAdd(&s.queue[2 * q + 1], 1u);
-        const int n = __ldg(s.lvl_leaf + c);
-        int nf = 0;
-        bool w3 = false, w4 = false;
+        // the next item: the next of this CTA's share (without level order) or
+        // the next in the queue, claimed now
+        unsigned cn = c + gridDim.x;
+        if (!fast && t == 0) cn = atomicAdd(&s.queue[2 * q + 1], 1u);
+        int n;
+        ItemRec r{};
         if (fast) {
-            rec(c, nf, w3, w4);
-            foreign_c<N>(s, c, w, nf, true, Fs);  // while the tile lands
+            r = item_rec_of(srec[st]);
+            n = r.n;
+            if ((int)cn < total) item_rec_stage(s, cn, q, srec[st ^ 1]);  // for the next item
+            foreign_c<N>(s, c, w, r.nf, true, Fs);                        // while the tile lands
+        } else {
+            n = __ldg(s.lvl_leaf + c);
         }
         if (__syncthreads_or(mbar_wait(&bar[st], (phase >> st) & 1u) ? 0 : 1)) {
             if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
@@ -1114,10 +1195,10 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         phase ^= 1u << st;
         double* T = tiles + (size_t)st * G.cplane;
         if (fast) {  // the ring, then Symmetric_C(2)_3/4, on the tile (and in memory if wr)
-            fill_ring_c<N>(s, G, c, n, w, 0, Fs, T, wr != 0);
+            fill_ring_c<N>(s, G, c, n, w, 0, r.na + r.nb, Fs, T, wr != 0);
             __syncthreads();
-            if (w3 || w4) {
-                wall_c_rows<N>(s, G, n, w, w3, w4, T, wr != 0);
+            if (r.w3 || r.w4) {
+                wall_c_rows<N>(s, G, n, w, r.w3, r.w4, T, wr != 0);
                 __syncthreads();
             }
         }
@@ -1125,10 +1206,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
             s_next = (int)cn;
             pend = ((int)cn < total) && !start_tile(st ^ 1, (int)cn, false);
         }
-        if (CONSUMER == CONS_MACRO_G)
-            err_reduce(s, n, macro_g_block<N>(s, G, n, T), red);
-        else
-            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED>(s, G, n, T);
+        consume(n, T);
         __syncthreads();
         c = s_next;
         st ^= 1;
@@ -1137,11 +1215,12 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
 }
 
 // Fill_Ghost_Cells_hg (Fill_Ghost_Cells_hg.f90:2-477) with Bounce_Back_3/4,
-// then streaming and Macroscopic_Values_h_AMR, one item per leaf in work
-// order. Each item bulk-copies its block's h and g planes into shared memory;
-// without level order (fast_fill) it fills its own ring there and in memory
-// and applies the walls; with level order the fill phase fills every leaf
-// first and the copy waits for the block's flag.
+// then streaming and Macroscopic_Values_h_AMR, one item per leaf. Each item
+// bulk-copies its block's h and g planes into shared memory. Without level
+// order (fast_fill) CTA b takes items b, b + gridDim.x, ..., fills each
+// item's ring on the staged planes (and in memory if wr), applies the walls
+// and streams; with level order the fill phase fills every leaf first and
+// consumer items come from a queue, their copy waiting for the block's flag.
 // Shared memory: mbarrier (128 bytes), h and g planes, the foreign values.
 template <int N>
 __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
@@ -1152,68 +1231,86 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
     const int q = Q_FILLHG;
     const int t = threadIdx.x;
     const int total = s.lvl_off[AMR_MAXLV];
-    const int lmin = s.cnt->level_min;
     const int FP = 9 * G.aplane;
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw);
     double* As = reinterpret_cast<double*>(smraw + 128);  // [h|g][q][pool plane layout]
     double* Fs = As + 2 * (size_t)FP;
-    const bool fast = fast_fill(s, q);
-    if (!fast)
-        fill_phase(
-            s, q, nbis, &s_next,
-            [&](int k, int n, const NbInfo& nbi) {
-                foreign_hg<N>(s, G, k, nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
-                if (nbi.wait[q]) {
-                    fill_ring_hg<N>(s, G, k, n, 1, Fs, nullptr);
-                    wait_coarse(s, q, nbi);
-                    fill_ring_hg<N>(s, G, k, n, 2, Fs, nullptr);
-                } else {
-                    fill_ring_hg<N>(s, G, k, n, 0, Fs, nullptr);
-                }
-            },
-            [&](int n, const NbInfo& nbi) { bounce_back<N>(s, G, n, nbi); });
     const unsigned fb = (unsigned)FP * 8;
-    const int* flags = fill_flags(s, q);
-    if (t == 0) {
-        mbar_init(bar, 1);
-        s_next = (int)atomicAdd(&s.queue[2 * q + 1], 1u);
+    auto copy_planes = [&](int nn) {  // thread 0
+        fence_proxy_async_all();
+        mbar_expect_tx(bar, 2 * fb);
+        bulk_g2s(As, s.Ah + (size_t)nn * FP, fb, bar);
+        bulk_g2s(As + FP, s.Ag + (size_t)nn * FP, fb, bar);
+    };
+    const bool fast = fast_fill(s, q);
+    if (t == 0) mbar_init(bar, 1);
+    __syncthreads();
+    unsigned phase = 0;
+
+    if (fast) {
+        __shared__ int srec[2][6];  // records of the current and the next item
+        int c = blockIdx.x, rb = 0;
+        if (c < total) item_rec_stage(s, c, q, srec[0]);
+        __syncthreads();
+        while (c < total) {
+            const int cn = c + gridDim.x;
+            const ItemRec r = item_rec_of(srec[rb]);
+            if (t == 0) copy_planes(r.n);
+            if (cn < total) item_rec_stage(s, cn, q, srec[rb ^ 1]);  // for the next iteration
+            foreign_hg<N>(s, G, c, r.nf, true, Fs);                  // while the planes land
+            if (__syncthreads_or(mbar_wait(bar, phase) ? 0 : 1)) {
+                if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
+                mbar_wait(bar, phase);  // the copies must land before exit
+                break;
+            }
+            phase ^= 1u;
+            // the ring, then Bounce_Back_3/4, on the staged planes (and in memory if wr)
+            fill_ring_hg<N>(s, G, c, r.n, 0, r.na, r.nb, Fs, As, wr != 0);
+            __syncthreads();
+            if (r.w3 || r.w4) {
+                bounce_back_staged<N>(s, G, r.n, r.w3, r.w4, As, wr != 0);
+                __syncthreads();
+            }
+            stream_block<N>(s, G, r.n, As);
+            __syncthreads();
+            c = cn;
+            rb ^= 1;
+        }
+        return;
     }
+
+    const int lmin = s.cnt->level_min;
+    fill_phase(
+        s, q, nbis, &s_next,
+        [&](int k, int n, const NbInfo& nbi) {
+            foreign_hg<N>(s, G, k, nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
+            if (nbi.wait[q]) {
+                fill_ring_hg<N>(s, G, k, n, 1, 0, 0, Fs, nullptr);
+                wait_coarse(s, q, nbi);
+                fill_ring_hg<N>(s, G, k, n, 2, 0, 0, Fs, nullptr);
+            } else {
+                fill_ring_hg<N>(s, G, k, n, 0, nbi.na[q], nbi.nb[q], Fs, nullptr);
+            }
+        },
+        [&](int n, const NbInfo& nbi) { bounce_back<N>(s, G, n, nbi); });
+    const int* flags = fill_flags(s, q);
+    if (t == 0) s_next = (int)atomicAdd(&s.queue[2 * q + 1], 1u);
     __syncthreads();
     int c = s_next;
-    unsigned phase = 0;
     while (c < total) {
-        unsigned cn = 0;
         const int n = __ldg(s.lvl_leaf + c);
         if (t == 0) {
-            cn = atomicAdd(&s.queue[2 * q + 1], 1u);
-            if (!fast && !spin_flag(flags + n)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
-            fence_proxy_async_all();
-            mbar_expect_tx(bar, 2 * fb);
-            bulk_g2s(As, s.Ah + (size_t)n * FP, fb, bar);
-            bulk_g2s(As + FP, s.Ag + (size_t)n * FP, fb, bar);
+            const unsigned cn = atomicAdd(&s.queue[2 * q + 1], 1u);
+            if (!spin_flag(flags + n)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
+            copy_planes(n);
             s_next = (int)cn;
-        }
-        bool w3 = false, w4 = false;
-        if (fast) {
-            const int* r = s.nbinfo + (size_t)c * NBI_STRIDE;
-            w3 = __ldg(r + 3) < 0;
-            w4 = __ldg(r + 4) < 0;
-            foreign_hg<N>(s, G, c, __ldg(r + REC_NF + q), true, Fs);  // while the planes land
         }
         if (__syncthreads_or(mbar_wait(bar, phase) ? 0 : 1)) {
             if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
-            mbar_wait(bar, phase);  // the copies must land before exit
+            mbar_wait(bar, phase);
             break;
         }
         phase ^= 1u;
-        if (fast) {  // the ring, then Bounce_Back_3/4, on the staged planes (and in memory if wr)
-            fill_ring_hg<N>(s, G, c, n, 0, Fs, As, wr != 0);
-            __syncthreads();
-            if (w3 || w4) {
-                bounce_back_staged<N>(s, G, n, w3, w4, As, wr != 0);
-                __syncthreads();
-            }
-        }
         stream_block<N>(s, G, n, As);
         c = s_next;
         __syncthreads();
