@@ -99,6 +99,15 @@ __device__ __forceinline__ double chem_pot_f(DV& dv, const PhysD& ph, double inv
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
+// Shared-memory load of data that stays unchanged while it is read (staged by
+// a completed bulk copy), issued where it is written in the source: the
+// collision then loads a population when it uses it instead of holding all
+// of them in registers.
+__device__ __forceinline__ double lds(const double* p) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)));
+    return v;
+}
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
                  : "memory");

@@ -749,19 +749,22 @@ __device__ void wall_c(const DevState& s, const Geo<N>& G, int n, const NbInfo& 
 
 // ---------------------------------------------------------------------------
 // Collision_h_g_AMR (LBM_Subroutines.f90:116-189) of cell c of block n.
-// T: shared C block (G.c(0,..)); the post-streaming populations B and (unless
-// FUSED) P, Ux, Uy are read from memory, where nothing writes them during the
+// T: shared C block (G.c(0,..)); Hb, Gb: the block's post-streaming h and g
+// planes (plane stride nx*ny; staged in shared memory or in memory); unless
+// FUSED, P, Ux, Uy are read from memory, where nothing writes them during the
 // launch. Writes the post-collision populations A to memory. FUSED: P, Ux,
 // Uy come from Macroscopic_Values_g_AMR (:205-240) evaluated here on the
 // same C ring.
-template <bool SAFE, bool FUSED, int N>
+template <bool SAFE, bool FUSED, bool SH, int N>
 __device__ __forceinline__ unsigned collide_cell(const DevState& s, const Geo<N>& G, int n, int c,
-                                                 double inv_dx, const double* T) {
+                                                 double inv_dx, const double* T, const double* Hb,
+                                                 const double* Gb) {
     const PhysD& ph = s.ph;
     const int nx = G.nx, BP = G.bplane, PP = G.pplane;
     const double inv_dx2 = inv_dx * inv_dx;
-    const double* Hn = s.Bh + (size_t)n * 9 * BP + c;
-    const double* Gn = s.Bg + (size_t)n * 9 * BP + c;
+    const double* Hn = Hb + c;
+    const double* Gn = Gb + c;
+    auto ldp = [&](const double* p) { return SH ? lds(p) : __ldg(p); };
     Div<SAFE> dv;
     {
         const int x = c % nx + 1, y = c / nx + 1;
@@ -795,7 +798,7 @@ __device__ __forceinline__ unsigned collide_cell(const DevState& s, const Geo<N>
             gradient_iso_f(dv, inv_dx, Cs, gx, gy);
             const double Fx = mu * gx;
             const double Fy = mu * gy + Fb;
-            auto g = [&](int k) { return __ldg(Gn + (k - 1) * BP); };
+            auto g = [&](int k) { return ldp(Gn + (k - 1) * BP); };
             const double sx = ((((g(2) - g(4)) + g(6)) - g(7)) - g(8)) + g(9);
             const double sy = ((((g(3) - g(5)) + g(6)) + g(7)) - g(8)) - g(9);
             const double rr = __drcp_rn(Rho);
@@ -835,12 +838,12 @@ __device__ __forceinline__ unsigned collide_cell(const DevState& s, const Geo<N>
             const double eN = (double)d_ex(k) * ni + (double)d_ey(k) * nj;
             const double Gm = wk * (1.0 + eU * (3.0 + 4.5 * eU) - U215);
             const double heq = c0 * (Gm + tmp * wk * eN);
-            s.Ah[G.a(n, k, x, y)] = __ldg(Hn + (k - 1) * BP) * ph.omwc + heq * ph.wc;
+            s.Ah[G.a(n, k, x, y)] = ldp(Hn + (k - 1) * BP) * ph.omwc + heq * ph.wc;
             const double Ak = (Gm - wk) * ph.dRho3 + Gm * mu;
             const double Bk = ((double)d_ey(k) - Uy) * Gm * Fb;
             const double hc = Ak * (Ec(k) - ud_c) + Bk;
             const double geq = P * wk + dv.d3((Gm - wk) * Rho) - 0.5 * hc;
-            f[k] = __ldg(Gn + (k - 1) * BP) - geq;
+            f[k] = ldp(Gn + (k - 1) * BP) - geq;
             hm[k] = Ak * (Em(k) - ud_m) + Bk;
         }
         // MRT_Collision_AMR (:348-361): Convert, relax 8 and 9, Reconvt, /36
@@ -868,26 +871,27 @@ __device__ __forceinline__ unsigned collide_cell(const DevState& s, const Geo<N>
         o[9] = b2 + 6.0 * m[4] + 3.0 * m[5] - 6.0 * m[6] - 3.0 * m[7] - 9.0 * m[9];
 #pragma unroll
         for (int k = 1; k <= 9; ++k)
-            s.Ag[G.a(n, k, x, y)] = (__ldg(Gn + (k - 1) * BP) - dv.d36(o[k])) + hm[k];
+            s.Ag[G.a(n, k, x, y)] = (ldp(Gn + (k - 1) * BP) - dv.d36(o[k])) + hm[k];
     }
     return dv.bad;
 }
 
 
 // Macroscopic_Values_g_AMR (LBM_Subroutines.f90:205-240) of cell c of block n
-// from T and the g populations in memory; dc = the Err_Interface term
-// (Refine_Derefine.f90:327-351) of the cell
-template <bool SAFE, int N>
+// from T and the block's g planes Gb (shared memory or memory); dc = the
+// Err_Interface term (Refine_Derefine.f90:327-351) of the cell
+template <bool SAFE, bool SH, int N>
 __device__ __forceinline__ unsigned macro_g_cell_f(const DevState& s, const Geo<N>& G, int n, int c,
-                                                   double inv_dx, const double* T, double& dc) {
+                                                   double inv_dx, const double* T, const double* Gb,
+                                                   double& dc) {
     const PhysD& ph = s.ph;
     const int nx = G.nx, BP = G.bplane;
     const double inv_dx2 = inv_dx * inv_dx;
     Div<SAFE> dv;
     const int x = c % nx + 1, y = c / nx + 1;
     auto Cs = [&](int a, int b) { return T[G.c(0, x + a, y + b)]; };
-    const double* Gn = s.Bg + (size_t)n * 9 * BP + c;
-    auto g = [&](int k) { return __ldg(Gn + (k - 1) * BP); };
+    const double* Gn = Gb + c;
+    auto g = [&](int k) { return SH ? lds(Gn + (k - 1) * BP) : __ldg(Gn + (k - 1) * BP); };
     double gx, gy;
     gradient_iso_f(dv, inv_dx, Cs, gx, gy);
     const double mu = chem_pot_f(dv, ph, inv_dx2, Cs);
@@ -913,26 +917,27 @@ __device__ __forceinline__ unsigned macro_g_cell_f(const DevState& s, const Geo<
 }
 // Collision of every cell of block n: the branch-free exact division path,
 // and the IEEE path for a cell whose flag says a quotient left its range.
-template <int N, bool FUSED>
+// SH: Hb and Gb point to shared memory (else to memory)
+template <int N, bool FUSED, bool SH>
 __device__ __forceinline__ void collide_block(const DevState& s, const Geo<N>& G, int n,
-                                              const double* T) {
+                                              const double* T, const double* Hb, const double* Gb) {
     const double inv_dx = 1.0 / (double)__ldg(s.dx + n);  // dx is a power of two: exact
     for (int c = threadIdx.x; c < G.nx * G.ny; c += blockDim.x)
-        if (collide_cell<false, FUSED>(s, G, n, c, inv_dx, T))
-            collide_cell<true, FUSED>(s, G, n, c, inv_dx, T);
+        if (collide_cell<false, FUSED, SH>(s, G, n, c, inv_dx, T, Hb, Gb))
+            collide_cell<true, FUSED, SH>(s, G, n, c, inv_dx, T, Hb, Gb);
 }
 
 // Macroscopic_Values_g_AMR of every cell of block n; returns this thread's
 // maximum of the Err_Interface terms
-template <int N>
+template <int N, bool SH>
 __device__ __forceinline__ double macro_g_block(const DevState& s, const Geo<N>& G, int n,
-                                                const double* T) {
+                                                const double* T, const double* Gb) {
     const double inv_dx = 1.0 / (double)__ldg(s.dx + n);
     double mx = 0.0;
     for (int c = threadIdx.x; c < G.nx * G.ny; c += blockDim.x) {
         double dc;
-        if (macro_g_cell_f<false>(s, G, n, c, inv_dx, T, dc))
-            macro_g_cell_f<true>(s, G, n, c, inv_dx, T, dc);
+        if (macro_g_cell_f<false, SH>(s, G, n, c, inv_dx, T, Gb, dc))
+            macro_g_cell_f<true, SH>(s, G, n, c, inv_dx, T, Gb, dc);
         mx = fmax(mx, dc);
     }
     return mx;
@@ -1082,7 +1087,20 @@ __device__ __forceinline__ ItemRec item_rec_of(const int* w) {
 // levels outside [LevelMin, LevelMax] are not filled, as the reference's DO
 // L = LevelMin, LevelMax, but still get the consumer work), and consumer
 // items are claimed from a queue, their tile copy waiting for the block's flag.
-// Shared memory: mbarriers (128 bytes), two C tiles, the foreign values.
+// Shared memory: mbarriers (128 bytes), two stages (C tile and, for the
+// consumer, the block's post-streaming h and / or g planes), the foreign
+// values.
+__host__ __device__ constexpr bool stage_h(int consumer) {
+    return consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED;
+}
+__host__ __device__ constexpr bool stage_g(int consumer) {
+    return stage_h(consumer) || consumer == CONS_MACRO_G;
+}
+// doubles of one stage: C tile, h planes, g planes
+__host__ __device__ inline size_t stage_doubles(int cplane, int bplane, int consumer) {
+    return (size_t)cplane + (stage_h(consumer) ? 9 * (size_t)bplane : 0) +
+           (stage_g(consumer) ? 9 * (size_t)bplane : 0);
+}
 template <int N, int CONSUMER>
 __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     k_fill_c(DevState s, int w, int q, int wr) {
@@ -1095,22 +1113,31 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     const int total = s.lvl_off[AMR_MAXLV];
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw);  // [2]
     double* tiles = reinterpret_cast<double*>(smraw + 128);
-    double* Fs = tiles + 2 * (size_t)G.cplane;
+    const size_t SD = stage_doubles(G.cplane, G.bplane, CONSUMER);
+    double* Fs = tiles + 2 * SD;
+    const size_t HP = 9 * (size_t)G.bplane;  // doubles of 9 planes
     const bool fast = fast_fill(s, q);
     constexpr bool collide = (CONSUMER == CONS_COLLIDE_READ || CONSUMER == CONS_COLLIDE_FUSED);
     if (collide && blockIdx.x == 0 && t == 0)
         atomicAdd(&s.cnt->updates, (unsigned long long)total * (unsigned long long)(G.nx * G.ny));
+    // stage st: C tile at tiles + st*SD, then h planes (if staged), then g planes
     auto consume = [&](int n, const double* T) {
+        const double* Hs = T + G.cplane;
+        const double* Gs = Hs + (stage_h(CONSUMER) ? HP : 0);
         if (CONSUMER == CONS_MACRO_G)
-            err_reduce(s, n, macro_g_block<N>(s, G, n, T), red);
+            err_reduce(s, n, macro_g_block<N, true>(s, G, n, T, Gs), red);
         else if (CONSUMER != CONS_NONE)
-            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED>(s, G, n, T);
+            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED, true>(s, G, n, T, Hs, Gs);
     };
-    const unsigned tb = (unsigned)G.cplane * 8;
+    const unsigned tb = (unsigned)G.cplane * 8, hb = (unsigned)HP * 8;
     auto copy_tile = [&](int st, int nn) {  // thread 0
+        double* T = tiles + st * SD;
         fence_proxy_async_all();
-        mbar_expect_tx(&bar[st], tb);
-        bulk_g2s(tiles + (size_t)st * G.cplane, s.C + (size_t)nn * G.cplane, tb, &bar[st]);
+        mbar_expect_tx(&bar[st], tb + (stage_h(CONSUMER) ? hb : 0) + (stage_g(CONSUMER) ? hb : 0));
+        bulk_g2s(T, s.C + (size_t)nn * G.cplane, tb, &bar[st]);
+        if (stage_h(CONSUMER)) bulk_g2s(T + G.cplane, s.Bh + (size_t)nn * HP, hb, &bar[st]);
+        if (stage_g(CONSUMER))
+            bulk_g2s(T + G.cplane + (stage_h(CONSUMER) ? HP : 0), s.Bg + (size_t)nn * HP, hb, &bar[st]);
     };
 
     const int lmin = s.cnt->level_min;
@@ -1193,7 +1220,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
             break;
         }
         phase ^= 1u << st;
-        double* T = tiles + (size_t)st * G.cplane;
+        double* T = tiles + st * SD;
         if (fast) {  // the ring, then Symmetric_C(2)_3/4, on the tile (and in memory if wr)
             fill_ring_c<N>(s, G, c, n, w, 0, r.na + r.nb, Fs, T, wr != 0);
             __syncthreads();
@@ -1337,7 +1364,8 @@ __global__ void __launch_bounds__(256, 2) k_collide(DevState s) {
     for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
         const int n = s.leaf[m];
         load_tile_c<N>(s, G, n, T);
-        collide_block<N, false>(s, G, n, T);
+        collide_block<N, false, false>(s, G, n, T, s.Bh + (size_t)n * 9 * G.bplane,
+                                s.Bg + (size_t)n * 9 * G.bplane);
         __syncthreads();
     }
 }
@@ -1351,7 +1379,7 @@ __global__ void __launch_bounds__(256, 2) k_macro_g(DevState s) {
     for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
         const int n = s.leaf[m];
         load_tile_c<N>(s, G, n, T);
-        err_reduce(s, n, macro_g_block<N>(s, G, n, T), red);
+        err_reduce(s, n, macro_g_block<N, false>(s, G, n, T, s.Bg + (size_t)n * 9 * G.bplane), red);
         __syncthreads();
     }
 }
@@ -1453,15 +1481,15 @@ int queue_grid(K kernel, int nt, size_t smem, const LaunchCfg& lc) {
     return lc.num_sms * occ;
 }
 
-// shared memory of a C-fill launch: mbarriers, two C tiles, foreign values
-size_t fill_c_smem(const DevState& s) {
-    return 128 + sizeof(double) * (2 * (size_t)s.cplane + (size_t)s.fmax);
+// shared memory of a C-fill launch: mbarriers, two stages, foreign values
+size_t fill_c_smem(const DevState& s, int consumer) {
+    return 128 + sizeof(double) * (2 * stage_doubles(s.cplane, s.bplane, consumer) + (size_t)s.fmax);
 }
 
 template <int N, int CONS>
 void fill_c_launch(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width, int q,
                    int wr) {
-    const size_t sm = fill_c_smem(s);
+    const size_t sm = fill_c_smem(s, CONS);
     const int nt = block_threads(s);
     smem_optin(k_fill_c<N, CONS>, sm);
     k_fill_c<N, CONS><<<queue_grid(k_fill_c<N, CONS>, nt, sm, lc), nt, sm, st>>>(s, width, q, wr);
