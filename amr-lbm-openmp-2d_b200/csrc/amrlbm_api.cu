@@ -485,7 +485,7 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     AL(ref_c1, int, NB);
     AL(der_list, int, NB);
     AL(cnt, Counters, 1);
-    AL(queue, unsigned, 2 * NQUEUES);
+    AL(queue, unsigned, 4 * NQUEUES);
     ctx->d_diag = dalloc<double>(ctx, 9 + 9 * NB, &e);
     if (e != cudaSuccess) {
         int r = cuda_fail(ctx, e, "cudaMalloc diag");
@@ -501,7 +501,7 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
         amrlbm_destroy(ctx);
         return AMRLBM_ERR_CUDA;
     }
-    // 1 KB tile per block fits the default 48 KB dynamic shared memory
+    launch_reset_queues(s, ctx->st);  // the level-ordered kernels start from zero counters
     cudaDeviceSynchronize();
     ctx->launches0 = launches_issued();
     *out = ctx;

@@ -40,7 +40,8 @@ struct Counters {
     int pad;
 };
 
-// Work queues of the level-ordered kernels: [2*q] = next item, [2*q+1] = items done.
+// Work queues of the level-ordered kernels (queue[4q..4q+2]: next fill item,
+// next consumer item, CTAs done; zero between launches).
 enum { Q_FILLC = 0, Q_FILLHG = 1, Q_FILLC1 = 2, NQUEUES = 3 };
 // per-leaf records of the level-ordered kernels, indexed by work-order
 // position: neighbour record (NBI_STRIDE ints) and one fill plan per ghost
@@ -84,7 +85,7 @@ struct DevState {
     int *freelist;   // ring buffer of the first ids of freed quartets
     int *ref_list, *ref_c1, *der_list;
     Counters* cnt;
-    unsigned* queue;  // [2*NQUEUES]
+    unsigned* queue;  // [4*NQUEUES]: per queue fill claims, consumer claims, CTAs done
     PhysD ph;
 };
 

@@ -693,7 +693,8 @@ long long launches_issued() { return g_launches; }
 void count_launches(int n) { g_launches += n; }
 
 void launch_reset_queues(const DevState& s, cudaStream_t st) {
-    cudaMemsetAsync(s.queue, 0, sizeof(unsigned) * 2 * NQUEUES, st);
+    cudaMemsetAsync(s.queue, 0, sizeof(unsigned) * 4 * NQUEUES, st);
+    cudaMemsetAsync(s.ring_done, 0, sizeof(int) * NQUEUES * (size_t)(s.max_blks + 1), st);
 }
 
 

@@ -429,13 +429,13 @@ __global__ void k_build_plans(DevState s) {
 // ---------------------------------------------------------------------------
 // Level-ordered launches, for fills that need level order: two phases in
 // one launch. Fill phase: CTAs claim fill items (one leaf's ghost ring) in
-// work order from queue[2q]. A fill item whose coarse-to-fine cells read a
+// work order from queue[4q]. A fill item whose coarse-to-fine cells read a
 // coarser neighbour's ring (other than its foreign cells) waits (bounded
 // spin) for that neighbour's flag; every fill item raises its own block's
 // flag when its ring, walls included, is in memory. Consumer phase: once the
 // fill queue is empty, CTAs claim consumer items (the work that needs the
 // block's own ring: collision, streaming, macroscopic values) from
-// queue[2q+1]; a consumer item waits only for its own block's flag. Without
+// queue[4q+1]; a consumer item waits only for its own block's flag. Without
 // level order there is no fill phase and consumer items fill their own rings.
 //
 // A CTA claims its next item as soon as it starts the current one (the
@@ -447,6 +447,29 @@ __global__ void k_build_plans(DevState s) {
 
 __device__ __forceinline__ int* fill_flags(const DevState& s, int q) {
     return s.ring_done + (size_t)q * (s.max_blks + 1);
+}
+
+// End of a level-ordered launch of queue q, called by every CTA: the last CTA
+// to finish clears the queue's counters and the flags of the leaves, for the
+// next launch. (Launches without level order use neither.)
+__device__ void queue_done(const DevState& s, int q) {
+    __shared__ int last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&s.queue[4 * q + 2], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    int* f = fill_flags(s, q);
+    const int total = s.lvl_off[AMR_MAXLV];
+    for (int k = threadIdx.x; k < total; k += blockDim.x) f[s.lvl_leaf[k]] = 0;
+    if (threadIdx.x == 0) {
+        s.queue[4 * q] = 0;
+        s.queue[4 * q + 1] = 0;
+        s.queue[4 * q + 2] = 0;
+    }
 }
 
 // bounded spin of one thread until *flag is set; false if it ran out
@@ -488,7 +511,7 @@ __device__ __forceinline__ void fill_phase(const DevState& s, int q, NbInfo* nbi
     const int lmin = s.cnt->level_min, lmax = s.cnt->level_max;
     const int total = s.lvl_off[AMR_MAXLV];
     const int t = threadIdx.x;
-    if (t == 0) *s_next = (int)atomicAdd(&s.queue[2 * q], 1u);
+    if (t == 0) *s_next = (int)atomicAdd(&s.queue[4 * q], 1u);
     __syncthreads();
     int k = *s_next;
     if (k < total && t < NBI_INTS)
@@ -498,7 +521,7 @@ __device__ __forceinline__ void fill_phase(const DevState& s, int q, NbInfo* nbi
     while (k < total) {
         const NbInfo& nbi = nbis[rb];
         unsigned kn = 0;
-        if (t == 0) kn = atomicAdd(&s.queue[2 * q], 1u);  // the next item, claimed now
+        if (t == 0) kn = atomicAdd(&s.queue[4 * q], 1u);  // the next item, claimed now
         const int n = nbi.id[0], L = nbi.lev[0];
         const bool do_fill = (L >= lmin && L <= lmax);
         if (do_fill) fill(k, n, nbi);
@@ -1168,6 +1191,8 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
                 if (r.w3 || r.w4) wall_c_rows<N>(s, G, r.n, w, r.w3, r.w4, nullptr);
                 __syncthreads();
             }
+        else
+            queue_done(s, q);
         return;
     }
     const int* flags = fill_flags(s, q);
@@ -1190,7 +1215,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     if (t == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
-        const int c0 = fast ? (int)blockIdx.x : (int)atomicAdd(&s.queue[2 * q + 1], 1u);
+        const int c0 = fast ? (int)blockIdx.x : (int)atomicAdd(&s.queue[4 * q + 1], 1u);
         s_next = c0;
         if (c0 < total) start_tile(0, c0, true);
     }
@@ -1203,7 +1228,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         // the next item: the next of this CTA's share (without level order) or
         // the next in the queue, claimed now
         unsigned cn = c + gridDim.x;
-        if (!fast && t == 0) cn = atomicAdd(&s.queue[2 * q + 1], 1u);
+        if (!fast && t == 0) cn = atomicAdd(&s.queue[4 * q + 1], 1u);
         int n;
         ItemRec r{};
         if (fast) {
@@ -1239,6 +1264,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         st ^= 1;
         if (t == 0 && pend) start_tile(st, c, true);
     }
+    if (!fast) queue_done(s, q);
 }
 
 // Fill_Ghost_Cells_hg (Fill_Ghost_Cells_hg.f90:2-477) with Bounce_Back_3/4,
@@ -1321,13 +1347,13 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
         },
         [&](int n, const NbInfo& nbi) { bounce_back<N>(s, G, n, nbi); });
     const int* flags = fill_flags(s, q);
-    if (t == 0) s_next = (int)atomicAdd(&s.queue[2 * q + 1], 1u);
+    if (t == 0) s_next = (int)atomicAdd(&s.queue[4 * q + 1], 1u);
     __syncthreads();
     int c = s_next;
     while (c < total) {
         const int n = __ldg(s.lvl_leaf + c);
         if (t == 0) {
-            const unsigned cn = atomicAdd(&s.queue[2 * q + 1], 1u);
+            const unsigned cn = atomicAdd(&s.queue[4 * q + 1], 1u);
             if (!spin_flag(flags + n)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
             copy_planes(n);
             s_next = (int)cn;
@@ -1342,6 +1368,7 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
         c = s_next;
         __syncthreads();
     }
+    queue_done(s, q);
 }
 
 // ---------------------------------------------------------------------------
@@ -1519,9 +1546,6 @@ void fill_c_dispatch(const DevState& s, const LaunchCfg& lc, cudaStream_t st, in
 void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width,
                    int consumer, int write_ring) {
     const int q = (width == 2) ? Q_FILLC : Q_FILLC1;
-    cudaMemsetAsync(s.queue + 2 * q, 0, 2 * sizeof(unsigned), st);
-    cudaMemsetAsync(s.ring_done + (size_t)q * (s.max_blks + 1), 0,
-                    sizeof(int) * (size_t)(s.max_blks + 1), st);
 #define C_(N) fill_c_dispatch<N>(s, lc, st, width, consumer, q, write_ring)
     DISPATCH(s, C_);
 #undef C_
@@ -1529,9 +1553,6 @@ void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int 
 }
 
 void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int write_ring) {
-    cudaMemsetAsync(s.queue + 2 * Q_FILLHG, 0, 2 * sizeof(unsigned), st);
-    cudaMemsetAsync(s.ring_done + (size_t)Q_FILLHG * (s.max_blks + 1), 0,
-                    sizeof(int) * (size_t)(s.max_blks + 1), st);
     const int nt = block_threads(s);
     // mbarrier, h and g planes, foreign values
     const size_t sm = 128 + 18 * sizeof(double) * ((size_t)s.aplane + (size_t)s.fmax);
