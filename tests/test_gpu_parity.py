@@ -215,3 +215,38 @@ def test_device_matches_golden_fixtures(name):
         assert snapshot(gpu, p) == want["init"]
         gpu.main_loop(steps)
         assert snapshot(gpu, p) == want["after_steps"]
+
+
+@pytest.mark.parametrize("case", ["reference_default", "small_16x16"])
+@pytest.mark.parametrize("narrow", ["finest_out", "coarsest_out"])
+def test_level_range_narrower_than_the_leaves(case, narrow):
+    """Fills over a level range that leaves some leaves out (the reference's
+    DO L = LevelMin, LevelMax with a narrower range): those leaves keep their
+    ghost cells and the rest read them as they are. This takes the
+    level-ordered path of the fill kernels."""
+    p = CASES[case]()
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    with AmrLbm(p) as gpu:
+        gpu.initialize_rising_bubble()
+        for step in range(2):
+            lo, hi = orc.determine_min_max_levels()
+            assert gpu.determine_min_max_levels() == (lo, hi)
+            if hi == lo:
+                pytest.skip("a single leaf level")
+            a, b = (lo, hi - 1) if narrow == "finest_out" else (lo + 1, hi)
+            orc.set_level_range(a, b)
+            gpu.set_level_range(a, b)
+            orc.fill_ghost_cells_c2()
+            gpu.fill_ghost_cells_c2()
+            compare_fields(gpu, orc, fields=("C",))
+            orc.phase_field_lbm_h_g()
+            gpu.phase_field_lbm_h_g()
+            compare_fields(gpu, orc, fields=("h", "g"))
+            orc.macroscopic_values_h()
+            gpu.macroscopic_values_h()
+            orc.fill_ghost_cells_c()
+            gpu.fill_ghost_cells_c()
+            orc.macroscopic_values_g()
+            gpu.macroscopic_values_g()
+            compare_state(gpu, orc)
