@@ -404,16 +404,24 @@ class AmrLbm:
         self._check(self.lib.amrlbm_upload_block(
             self.ctx, bid, *[_ptr(a, ct.c_double) for a in arrs]))
 
-    def download_fields(self, ids):
+    def download_fields(self, ids, out=None):
         """Fields of blocks `ids` as flat per-block records (n, size) in the
-        reference's column-major layouts; reshape a record with order="F"."""
+        reference's column-major layouts; reshape a record with order="F".
+        `out`: arrays to fill (C-contiguous float64 of those shapes, e.g. in
+        page-locked memory), else new ones."""
         ids = np.ascontiguousarray(ids, dtype=np.int32)
         n = len(ids)
         hs = int(np.prod(self.hshape))
         cs = int(np.prod(self.cshape))
         ps = int(np.prod(self.pshape))
-        out = dict(h=np.zeros((n, hs)), g=np.zeros((n, hs)), C=np.zeros((n, cs)),
-                   P=np.zeros((n, ps)), Ux=np.zeros((n, ps)), Uy=np.zeros((n, ps)))
+        if out is None:
+            out = dict(h=np.zeros((n, hs)), g=np.zeros((n, hs)), C=np.zeros((n, cs)),
+                       P=np.zeros((n, ps)), Ux=np.zeros((n, ps)), Uy=np.zeros((n, ps)))
+        want = dict(h=hs, g=hs, C=cs, P=ps, Ux=ps, Uy=ps)
+        for k, sz in want.items():
+            a = out[k]
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape != (n, sz):
+                raise ValueError(f"out[{k!r}] must be C-contiguous float64 of shape {(n, sz)}")
         self._check(self.lib.amrlbm_download_fields(
             self.ctx, n, _ptr(ids, ct.c_int32),
             *[_ptr(out[k], ct.c_double) for k in ("h", "g", "C", "P", "Ux", "Uy")]))

@@ -53,8 +53,6 @@ struct amrlbm_ctx {
     long long launches0 = 0;
     long long captured = 0, replayed = 0;  // graph kernels: captured once, run per replay
     GraphEntry* prof_pending = nullptr;    // replayed with profiling, events not read yet
-    double* h_stage = nullptr;             // pinned host staging
-    size_t h_stage_doubles = 0;
 };
 
 namespace {
@@ -113,38 +111,40 @@ PhysD to_physd(const amrlbm_physics& p) {
 }
 
 // ---- field transfer kernels (reference layouts <-> pool layouts) ----------
-// per block record offsets in the staging buffer
-struct StageLayout {
-    size_t h, g, C, P, Ux, Uy, per;
+
+// Field offsets of a transfer of n blocks, field by field (h, g, C, P, Ux,
+// Uy; -1: not transferred): field f of block i is at off[f] + i*size(f) of
+// the staging buffer, in the reference's per-block layout.
+struct XferLayout {
+    long long off[6];
+    size_t size[6], total;
 };
-StageLayout stage_layout(int nx, int ny) {
-    StageLayout L;
+XferLayout xfer_layout(int nx, int ny, int n, const void* const* fields) {
+    XferLayout X;
     const size_t hs = (size_t)9 * (nx + 2) * (ny + 2), cs = (size_t)(nx + 4) * (ny + 4),
                  ps = (size_t)nx * ny;
-    L.h = 0;
-    L.g = hs;
-    L.C = 2 * hs;
-    L.P = 2 * hs + cs;
-    L.Ux = L.P + ps;
-    L.Uy = L.Ux + ps;
-    L.per = L.Uy + ps;
-    return L;
+    const size_t sz[6] = {hs, hs, cs, ps, ps, ps};
+    X.total = 0;
+    for (int f = 0; f < 6; ++f) {
+        X.size[f] = sz[f];
+        X.off[f] = fields[f] ? (long long)X.total : -1;
+        if (fields[f]) X.total += (size_t)n * sz[f];
+    }
+    return X;
 }
 
-// dir 0: staging (reference layout) -> pool; 1: pool -> staging. mask bits: h g C P Ux Uy
-__global__ void k_transfer(DevState s, const int* ids, int n, double* stage, int dir, int mask,
-                           StageLayout L) {
+// dir 0: staging -> pool; 1: pool -> staging (layout of xfer_layout)
+__global__ void k_transfer(DevState s, const int* ids, int n, double* stage, int dir,
+                           XferLayout X) {
     const int nx = s.nx, ny = s.ny;
-    const int hs = 9 * (nx + 2) * (ny + 2), cs = (nx + 4) * (ny + 4), ps = nx * ny;
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
         const int b = ids[i];
-        double* rec = stage + (size_t)i * L.per;
         for (int f = 0; f < 2; ++f) {
-            if (!(mask & (1 << f))) continue;
+            if (X.off[f] < 0) continue;
             double* A = f ? s.Ag : s.Ah;
             double* B = f ? s.Bg : s.Bh;
-            double* r = rec + (f ? L.g : L.h);
-            for (int e = threadIdx.x; e < hs; e += blockDim.x) {
+            double* r = stage + X.off[f] + (size_t)i * X.size[f];
+            for (int e = threadIdx.x; e < (int)X.size[f]; e += blockDim.x) {
                 const int q = e % 9 + 1, xy = e / 9, x = xy % (nx + 2), y = xy / (nx + 2);
                 const bool in = x >= 1 && x <= nx && y >= 1 && y <= ny;
                 double* p = in ? &B[b_idx(s, b, q, x, y)] : &A[a_idx(s, b, q, x, y)];
@@ -154,54 +154,49 @@ __global__ void k_transfer(DevState s, const int* ids, int n, double* stage, int
                     r[e] = *p;
             }
         }
-        if (mask & 4)
-            for (int e = threadIdx.x; e < cs; e += blockDim.x) {
-                const int x = e % (nx + 4) - 1, y = e / (nx + 4) - 1;
-                double* p = &s.C[c_idx(s, b, x, y)];
+        if (X.off[2] >= 0) {
+            double* r = stage + X.off[2] + (size_t)i * X.size[2];
+            for (int e = threadIdx.x; e < (int)X.size[2]; e += blockDim.x) {
+                double* p = &s.C[c_idx(s, b, e % (nx + 4) - 1, e / (nx + 4) - 1)];
                 if (dir == 0)
-                    *p = rec[L.C + e];
+                    *p = r[e];
                 else
-                    rec[L.C + e] = *p;
+                    r[e] = *p;
             }
+        }
         for (int f = 0; f < 3; ++f) {
-            if (!(mask & (8 << f))) continue;
+            if (X.off[3 + f] < 0) continue;
             double* A = f == 0 ? s.P : (f == 1 ? s.Ux : s.Uy);
-            const size_t off = f == 0 ? L.P : (f == 1 ? L.Ux : L.Uy);
-            for (int e = threadIdx.x; e < ps; e += blockDim.x) {
+            double* r = stage + X.off[3 + f] + (size_t)i * X.size[3 + f];
+            for (int e = threadIdx.x; e < (int)X.size[3 + f]; e += blockDim.x) {
                 double* p = &A[(size_t)b * s.pplane + e];
                 if (dir == 0)
-                    *p = rec[off + e];
+                    *p = r[e];
                 else
-                    rec[off + e] = *p;
+                    r[e] = *p;
             }
         }
     }
 }
 
-int ensure_stage(amrlbm_ctx* ctx, size_t nblocks) {
-    const StageLayout L = stage_layout(ctx->prm.nx, ctx->prm.ny);
-    // grow geometrically: the leaf count changes at every regrid
-    if (nblocks * L.per > ctx->stage_doubles || nblocks * L.per > ctx->h_stage_doubles)
-        nblocks = nblocks + nblocks / 2 + 16;
-    if (nblocks > (size_t)ctx->prm.max_blks) nblocks = (size_t)ctx->prm.max_blks;
-    const size_t need = nblocks * L.per;
-    if (need > ctx->stage_doubles) {
+// device staging of at least `doubles` doubles and `nblocks` block ids;
+// grows geometrically (the leaf count changes at every regrid)
+int ensure_stage(amrlbm_ctx* ctx, size_t doubles, size_t nblocks) {
+    if (doubles > ctx->stage_doubles) {
+        const size_t need = doubles + doubles / 2 + 4096;
         if (ctx->d_stage) cudaFree(ctx->d_stage);
         ctx->d_stage = nullptr;
+        ctx->stage_doubles = 0;
         CK(cudaMalloc(&ctx->d_stage, need * sizeof(double)));
         ctx->stage_doubles = need;
     }
-    if (need > ctx->h_stage_doubles) {
-        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
-        ctx->h_stage = nullptr;
-        CK(cudaMallocHost(&ctx->h_stage, need * sizeof(double)));
-        ctx->h_stage_doubles = need;
-    }
     if (nblocks > ctx->ids_cap) {
+        const size_t need = nblocks + nblocks / 2 + 16;
         if (ctx->d_ids) cudaFree(ctx->d_ids);
         ctx->d_ids = nullptr;
-        CK(cudaMalloc(&ctx->d_ids, nblocks * sizeof(int)));
-        ctx->ids_cap = nblocks;
+        ctx->ids_cap = 0;
+        CK(cudaMalloc(&ctx->d_ids, need * sizeof(int)));
+        ctx->ids_cap = need;
     }
     return 0;
 }
@@ -522,7 +517,6 @@ int amrlbm_destroy(amrlbm_ctx* ctx) {
     if (ctx->d_stage) cudaFree(ctx->d_stage);
     if (ctx->d_ids) cudaFree(ctx->d_ids);
     if (ctx->d_flush) cudaFree(ctx->d_flush);
-    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     if (ctx->t0) cudaEventDestroy(ctx->t0);
     if (ctx->t1) cudaEventDestroy(ctx->t1);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -727,28 +721,19 @@ int amrlbm_download_fields(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, doubl
     if (n == 0) return AMRLBM_OK;
     for (int i = 0; i < n; ++i)
         if (ids[i] < 1 || ids[i] > ctx->prm.max_blks) return AMRLBM_ERR_ARG;
-    if (int r = ensure_stage(ctx, (size_t)n)) return r;
-    const StageLayout L = stage_layout(ctx->prm.nx, ctx->prm.ny);
-    const int mask = (h ? 1 : 0) | (g ? 2 : 0) | (C ? 4 : 0) | (P ? 8 : 0) | (Ux ? 16 : 0) |
-                     (Uy ? 32 : 0);
+    double* dst[6] = {h, g, C, P, Ux, Uy};
+    const void* fl[6] = {h, g, C, P, Ux, Uy};
+    const XferLayout X = xfer_layout(ctx->prm.nx, ctx->prm.ny, n, fl);
+    if (X.total == 0) return AMRLBM_OK;
+    if (int r = ensure_stage(ctx, X.total, (size_t)n)) return r;
     CK(cudaMemcpyAsync(ctx->d_ids, ids, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->st));
-    k_transfer<<<ctx->lc.grid_leaves, 256, 0, ctx->st>>>(ctx->s, ctx->d_ids, n, ctx->d_stage, 1,
-                                                         mask, L);
+    k_transfer<<<ctx->lc.grid_leaves, 256, 0, ctx->st>>>(ctx->s, ctx->d_ids, n, ctx->d_stage, 1, X);
     CK(cudaGetLastError());
-    double* host = ctx->h_stage;
-    CK(cudaMemcpyAsync(host, ctx->d_stage, (size_t)n * L.per * 8, cudaMemcpyDeviceToHost,
-                       ctx->st));
+    for (int f = 0; f < 6; ++f)  // straight into the caller's arrays
+        if (dst[f])
+            CK(cudaMemcpyAsync(dst[f], ctx->d_stage + X.off[f], (size_t)n * X.size[f] * 8,
+                               cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    const size_t hs = L.g - L.h, cs = L.P - L.C, ps = L.Ux - L.P;
-    for (int i = 0; i < n; ++i) {
-        const double* rec = host + (size_t)i * L.per;
-        if (h) std::memcpy(h + i * hs, rec + L.h, hs * 8);
-        if (g) std::memcpy(g + i * hs, rec + L.g, hs * 8);
-        if (C) std::memcpy(C + i * cs, rec + L.C, cs * 8);
-        if (P) std::memcpy(P + i * ps, rec + L.P, ps * 8);
-        if (Ux) std::memcpy(Ux + i * ps, rec + L.Ux, ps * 8);
-        if (Uy) std::memcpy(Uy + i * ps, rec + L.Uy, ps * 8);
-    }
     return device_error(ctx);
 }
 
@@ -845,9 +830,8 @@ int amrlbm_init_rising_bubble(amrlbm_ctx* ctx) {
     {
         std::vector<int> ids(nb);
         for (int n = 1; n <= nb; ++n) ids[n - 1] = n;
-        const StageLayout L = stage_layout(p.nx, p.ny);
-        std::vector<double> z((size_t)nb * (L.per));
-        const size_t hs = L.g - L.h, cs = L.P - L.C, ps = L.Ux - L.P;
+        const size_t hs = (size_t)9 * (p.nx + 2) * (p.ny + 2), cs = (size_t)(p.nx + 4) * (p.ny + 4),
+                     ps = (size_t)p.nx * p.ny;
         std::vector<double> zh(nb * hs, 0.0), zc(nb * cs, 0.0), zp(nb * ps, 0.0);
         if (int r = upload_blocks(ctx, nb, ids.data(), zh.data(), zh.data(), zc.data(), zp.data(),
                                   zp.data(), zp.data()))
@@ -1069,26 +1053,17 @@ int upload_blocks(amrlbm_ctx* ctx, int n, const int* ids, const double* h, const
                   const double* C, const double* P, const double* Ux, const double* Uy) {
     for (int i = 0; i < n; ++i)
         if (ids[i] < 1 || ids[i] > ctx->prm.max_blks) return AMRLBM_ERR_ARG;
-    if (int r = ensure_stage(ctx, (size_t)n)) return r;
-    const StageLayout L = stage_layout(ctx->prm.nx, ctx->prm.ny);
-    const int mask = (h ? 1 : 0) | (g ? 2 : 0) | (C ? 4 : 0) | (P ? 8 : 0) | (Ux ? 16 : 0) |
-                     (Uy ? 32 : 0);
-    double* host = ctx->h_stage;
-    const size_t hs = L.g - L.h, cs = L.P - L.C, ps = L.Ux - L.P;
-    for (int i = 0; i < n; ++i) {
-        double* rec = host + (size_t)i * L.per;
-        if (h) std::memcpy(rec + L.h, h + i * hs, hs * 8);
-        if (g) std::memcpy(rec + L.g, g + i * hs, hs * 8);
-        if (C) std::memcpy(rec + L.C, C + i * cs, cs * 8);
-        if (P) std::memcpy(rec + L.P, P + i * ps, ps * 8);
-        if (Ux) std::memcpy(rec + L.Ux, Ux + i * ps, ps * 8);
-        if (Uy) std::memcpy(rec + L.Uy, Uy + i * ps, ps * 8);
-    }
-    CK(cudaMemcpyAsync(ctx->d_stage, host, (size_t)n * L.per * 8, cudaMemcpyHostToDevice,
-                       ctx->st));
+    const double* src[6] = {h, g, C, P, Ux, Uy};
+    const void* fl[6] = {h, g, C, P, Ux, Uy};
+    const XferLayout X = xfer_layout(ctx->prm.nx, ctx->prm.ny, n, fl);
+    if (X.total == 0) return 0;
+    if (int r = ensure_stage(ctx, X.total, (size_t)n)) return r;
+    for (int f = 0; f < 6; ++f)  // straight from the caller's arrays
+        if (src[f])
+            CK(cudaMemcpyAsync(ctx->d_stage + X.off[f], src[f], (size_t)n * X.size[f] * 8,
+                               cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->d_ids, ids, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->st));
-    k_transfer<<<ctx->lc.grid_leaves, 256, 0, ctx->st>>>(ctx->s, ctx->d_ids, n, ctx->d_stage, 0,
-                                                         mask, L);
+    k_transfer<<<ctx->lc.grid_leaves, 256, 0, ctx->st>>>(ctx->s, ctx->d_ids, n, ctx->d_stage, 0, X);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->st));  // the staging buffer is reused by the next call
     return 0;
