@@ -56,7 +56,9 @@ struct NbInfo {
     int bi, bj;
     int wait[NQUEUES];
     int nf[NQUEUES];
-    int na[NQUEUES], nb[NQUEUES];  // plan entries of kinds 1/-1 and 2/3 (stored first)
+    // plan entries stored first: na of kinds 1 and -1, then n2 of kind 2, then
+    // n3 of kind 3 (then those without a plan)
+    int na[NQUEUES], n2[NQUEUES], n3[NQUEUES];
 };
 constexpr int NBI_INTS = (int)(sizeof(NbInfo) / sizeof(int));
 static_assert(NBI_INTS <= NBI_STRIDE, "NbInfo record");
@@ -173,6 +175,11 @@ __device__ __forceinline__ void plan_store(int* base, int R, int t, const GPlan&
     for (int i = 0; i < 9; ++i) base[(1 + i) * R + t] = (i < ns) ? (int)(unsigned)P.src[i] : 0;
 }
 __device__ __forceinline__ int plan_kind(int meta) { return (meta & 7) - 1; }
+// storage class of a plan entry: 0 copy or level jump, 1 fine-to-coarse,
+// 2 coarse-to-fine, 3 no plan
+__device__ __forceinline__ int plan_class(int kind) {
+    return (kind == 1 || kind < 0) ? 0 : (kind == 2 ? 1 : (kind == 3 ? 2 : 3));
+}
 
 // Biquadratic_from_Fine / _Coarse (Interpolations.f90:2-138) at one output
 // point from its 9 gathered sources g[3*r+c]: first along the reference's
@@ -276,13 +283,13 @@ __device__ void load_nbinfo(const DevState& s, int n, NbInfo& r) {
 // plan is the same in the C2, C1 and h/g fills (only the offsets differ, C
 // pool or A pool), and a leaf's foreign cells are shared by the three.
 template <int N>
-__global__ void k_build_plans(DevState s) {
+__global__ void __launch_bounds__(128, 8) k_build_plans(DevState s) {
     const Geo<N> G(s);
     extern __shared__ int tab[];  // [9][ring1_len]: foreign cell -> slot
     __shared__ NbInfo nbi;
     __shared__ NbInfo cnb[9];     // coarser neighbours' records
     __shared__ int nfs;
-    __shared__ int cls_n[2][3], cls_f[2][3];  // [C2 | ring-1 plans][class]: count, fill
+    __shared__ int cls_n[2][4], cls_f[2][4];  // [C2 | ring-1 plans][class]: count, fill
     const int nx = G.nx, ny = G.ny, R2 = ring2_len(nx, ny), R1 = ring1_len(nx, ny);
     const int total = s.lvl_off[AMR_MAXLV];
     const int t = threadIdx.x, fmax = s.fmax;
@@ -292,9 +299,9 @@ __global__ void k_build_plans(DevState s) {
             load_nbinfo(s, n, nbi);
             nfs = 0;
         }
-        if (t < 6) {
-            cls_n[t / 3][t % 3] = 0;
-            cls_f[t / 3][t % 3] = 0;
+        if (t < 8) {
+            cls_n[t / 4][t % 4] = 0;
+            cls_f[t / 4][t % 4] = 0;
         }
         for (int i = t; i < 9 * R1; i += blockDim.x) tab[i] = -1;
         __syncthreads();
@@ -333,9 +340,9 @@ __global__ void k_build_plans(DevState s) {
                            return 0;
                        },
                        P);
-            // entries are stored by class: copies and level jumps, interpolated
-            // cells, cells without a plan
-            const int cls = (P.kind == 1 || P.kind < 0) ? 0 : (P.kind >= 2 ? 1 : 2);
+            // entries are stored by class: copies and level jumps,
+            // fine-to-coarse cells, coarse-to-fine cells, cells without a plan
+            const int cls = plan_class(P.kind);
             atomicAdd(&cls_n[0][cls], 1);
             if (r1) atomicAdd(&cls_n[1][cls], 1);
             if (P.kind < 0) {  // the level jump is reported by the level-ordered fills
@@ -381,7 +388,8 @@ __global__ void k_build_plans(DevState s) {
             nbi.nf[t] = nfs;
             const int pt = (t == Q_FILLC) ? 0 : 1;
             nbi.na[t] = cls_n[pt][0];
-            nbi.nb[t] = cls_n[pt][1];
+            nbi.n2[t] = cls_n[pt][1];
+            nbi.n3[t] = cls_n[pt][2];
             if (nbi.wait[t]) atomicOr(&s.fillinfo[t], 1);
         }
         // 3: the plans, foreign cells by slot
@@ -406,10 +414,11 @@ __global__ void k_build_plans(DevState s) {
                            return w;
                        },
                        P);
-            const int cls = (P.kind == 1 || P.kind < 0) ? 0 : (P.kind >= 2 ? 1 : 2);
+            const int cls = plan_class(P.kind);
             auto slot = [&](int pt) {
-                return (cls > 0 ? cls_n[pt][0] : 0) + (cls > 1 ? cls_n[pt][1] : 0) +
-                       atomicAdd(&cls_f[pt][cls], 1);
+                int base = 0;
+                for (int m = 0; m < cls; ++m) base += cls_n[pt][m];
+                return base + atomicAdd(&cls_f[pt][cls], 1);
             };
             plan_store(s.plan_c2 + (size_t)k * R2 * PLAN_INTS, R2, slot(0), P, i);
             if (x >= 0 && x <= nx + 1 && y >= 0 && y <= ny + 1) {
@@ -623,49 +632,58 @@ __device__ __forceinline__ bool pass_takes(int mode, int kind) {
     return mode == 0 || ((kind == 3) == (mode == 2));
 }
 
-// C ghost ring of width w of item k (block n) from its plans, into memory
-// (unless to_mem is false) and, if T is given, into the block's shared C tile
-// (index G.c(0,x,y)). Kind 1 and 2 sources are interiors no launch of this
-// fill writes. The plan entries are stored by class (copies, interpolated
-// cells, cells without a plan): pass 0 visits only the first na + nb.
+// One C ghost cell: plan entry e (plan array pl, ring length R, width w) of
+// block n, into memory (unless to_mem is false) and, if T is given, into the
+// block's shared C tile (index G.c(0,x,y)). Kind 1 and 2 sources are
+// interiors no launch of this fill writes; kind 3 sources are foreign slots
+// (Fs) or cells in memory. Returns the kind.
+template <int N>
+__device__ __forceinline__ int c_entry(const DevState& s, const Geo<N>& G, const int* pl, int R,
+                                       int e, int n, int w, const double* Fs, double* T,
+                                       bool to_mem) {
+    const int meta = __ldg(pl + e);
+    const int kind = plan_kind(meta);
+    if (kind == 0) return 0;
+    int x, y;
+    if (w == 2)
+        ring2_xy(meta >> 8, G.nx, G.ny, x, y);
+    else
+        ring1_xy(meta >> 8, G.nx, G.ny, x, y);
+    if (kind < 0) {
+        set_error(s, 4 /*AMRLBM_ERR_LEVEL_JUMP*/, n);
+        return kind;
+    }
+    double v;
+    if (kind == 1) {
+        v = __ldg(s.C + (unsigned)__ldg(pl + R + e));
+    } else {
+        double g[9];
+        if (kind == 2) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)__ldg(pl + (1 + i) * R + e));
+        } else {
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                g[i] = c2f_source((unsigned)__ldg(pl + (1 + i) * R + e), Fs, s.C, 0);
+        }
+        v = plan_combine(meta, g);
+    }
+    if (to_mem) s.C[G.c(n, x, y)] = v;
+    if (T) T[G.c(0, x, y)] = v;
+    return kind;
+}
+
+// C ghost ring of width w of item k (block n), level-ordered path, into
+// memory: pass 0 all plan entries, 1 all but coarse-to-fine (before a
+// wait), 2 coarse-to-fine only (after it). The foreign cells are in Fs.
 template <int N>
 __device__ void fill_ring_c(const DevState& s, const Geo<N>& G, int k, int n, int w, int mode,
-                            int nab, const double* Fs, double* T, bool to_mem = true) {
-    const int nx = G.nx, ny = G.ny;
-    const int R = (w == 2) ? ring2_len(nx, ny) : ring1_len(nx, ny);
+                            const double* Fs) {
+    const int R = (w == 2) ? ring2_len(G.nx, G.ny) : ring1_len(G.nx, G.ny);
     const int* pl = ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)k * R * PLAN_INTS;
-    const int lim = (mode == 0) ? nab : R;
-    for (int e = threadIdx.x; e < lim; e += blockDim.x) {
-        const int meta = __ldg(pl + e);
-        const int kind = plan_kind(meta);
-        if (kind == 0 || !pass_takes(mode, kind)) continue;
-        int x, y;
-        if (w == 2)
-            ring2_xy(meta >> 8, nx, ny, x, y);
-        else
-            ring1_xy(meta >> 8, nx, ny, x, y);
-        if (kind < 0) {
-            set_error(s, 4 /*AMRLBM_ERR_LEVEL_JUMP*/, n);
-            continue;
-        }
-        double v;
-        if (kind == 1) {
-            v = __ldg(s.C + (unsigned)__ldg(pl + R + e));
-        } else {
-            double g[9];
-            if (kind == 2) {
-#pragma unroll
-                for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)__ldg(pl + (1 + i) * R + e));
-            } else {
-#pragma unroll
-                for (int i = 0; i < 9; ++i)
-                    g[i] = c2f_source((unsigned)__ldg(pl + (1 + i) * R + e), Fs, s.C, 0);
-            }
-            v = plan_combine(meta, g);
-        }
-        if (to_mem) s.C[G.c(n, x, y)] = v;
-        if (T) T[G.c(0, x, y)] = v;
-    }
+    for (int e = threadIdx.x; e < R; e += blockDim.x)
+        if (pass_takes(mode, plan_kind(__ldg(pl + e))))
+            c_entry<N>(s, G, pl, R, e, n, w, Fs, nullptr, true);
 }
 
 // One copied h/g ghost cell (plan entry e, field f): the 9 populations'
@@ -721,35 +739,22 @@ __device__ __forceinline__ void hg_interp(const DevState& s, const Geo<N>& G, co
     }
 }
 
-// h/g ghost ring of item k (block n) from its plans, into memory (unless
-// to_mem is false) and, if As is given, into the block's staged planes
-// ([field][q][pool plane layout]). A cell without a plan keeps its value in
-// memory. Pass 0 runs its na copies (per field) and nb interpolated cells
-// (per population) as one set of units; passes 1 and 2 filter all entries.
+// h/g ghost ring of item k (block n), level-ordered path, into memory (pass
+// as fill_ring_c). A cell without a plan keeps its value in memory.
 template <int N>
-__device__ void fill_ring_hg(const DevState& s, const Geo<N>& G, int k, int n, int mode, int na,
-                             int nb, const double* Fs, double* As, bool to_mem = true) {
+__device__ void fill_ring_hg(const DevState& s, const Geo<N>& G, int k, int n, int mode,
+                             const double* Fs) {
     const int RG = ring1_len(G.nx, G.ny);
     const int* pl = s.plan_hg + (size_t)k * RG * PLAN_INTS;
-    if (mode == 0) {
-        for (int u = threadIdx.x; u < 2 * na + 9 * nb; u += blockDim.x) {
-            if (u < 2 * na)
-                hg_copy<N>(s, G, pl, RG, u % na, u / na, n, As, to_mem);
-            else
-                hg_interp<N>(s, G, pl, RG, na + (u - 2 * na) % nb, (u - 2 * na) / nb, n, Fs, As,
-                             to_mem);
-        }
-        return;
-    }
-    if (mode == 1)
+    if (mode != 2)
         for (int u = threadIdx.x; u < 2 * RG; u += blockDim.x) {
             const int kind = plan_kind(__ldg(pl + u % RG));
-            if (kind == 1 || kind == -1) hg_copy<N>(s, G, pl, RG, u % RG, u / RG, n, As, to_mem);
+            if (kind == 1 || kind == -1) hg_copy<N>(s, G, pl, RG, u % RG, u / RG, n, nullptr, true);
         }
     for (int u = threadIdx.x; u < 9 * RG; u += blockDim.x) {
         const int kind = plan_kind(__ldg(pl + u % RG));
         if (kind >= 2 && pass_takes(mode, kind))
-            hg_interp<N>(s, G, pl, RG, u % RG, u / RG, n, Fs, As, to_mem);
+            hg_interp<N>(s, G, pl, RG, u % RG, u / RG, n, Fs, nullptr, true);
     }
 }
 
@@ -1072,20 +1077,27 @@ __host__ __device__ constexpr int fill_c_min_blocks(int consumer) {
 // word offsets in a neighbour record
 constexpr int REC_NF = (int)(offsetof(NbInfo, nf) / sizeof(int));
 constexpr int REC_NA = (int)(offsetof(NbInfo, na) / sizeof(int));
-constexpr int REC_NB = (int)(offsetof(NbInfo, nb) / sizeof(int));
+constexpr int REC_N2 = (int)(offsetof(NbInfo, n2) / sizeof(int));
+constexpr int REC_N3 = (int)(offsetof(NbInfo, n3) / sizeof(int));
 
 // what an item of fill q needs from its record: block, foreign cells, plan
-// entry classes, walls (id[3], id[4] < 0)
+// entry classes, walls (id[3], id[4] < 0); staged in shared memory by
+// threads 0..6 (REC_WORDS words), read from there by every thread
 struct ItemRec {
-    int n, nf, na, nb;
+    int n, nf, na, n2, n3;
     bool w3, w4;
 };
-// the same words staged in shared memory by threads 0..5 (ItemRec from there)
+constexpr int REC_WORDS = 7;
 __device__ __forceinline__ void item_rec_stage(const DevState& s, int c, int q, int* dst) {
     const int t = threadIdx.x;
-    if (t < 6) {
-        // n, nf, na, nb, id[3] (bottom), id[4] (top)
-        const int off = t == 0 ? 0 : t == 1 ? REC_NF + q : t == 2 ? REC_NA + q : t == 3 ? REC_NB + q : t - 1;
+    if (t < REC_WORDS) {
+        // n, nf, na, n2, n3, id[3] (bottom), id[4] (top)
+        const int off = t == 0   ? 0
+                        : t == 1 ? REC_NF + q
+                        : t == 2 ? REC_NA + q
+                        : t == 3 ? REC_N2 + q
+                        : t == 4 ? REC_N3 + q
+                                 : t - 2;
         dst[t] = __ldg(s.nbinfo + (size_t)c * NBI_STRIDE + off);
     }
 }
@@ -1094,10 +1106,44 @@ __device__ __forceinline__ ItemRec item_rec_of(const int* w) {
     o.n = w[0];
     o.nf = w[1];
     o.na = w[2];
-    o.nb = w[3];
-    o.w3 = w[4] < 0;
-    o.w4 = w[5] < 0;
+    o.n2 = w[3];
+    o.n3 = w[4];
+    o.w3 = w[5] < 0;
+    o.w4 = w[6] < 0;
     return o;
+}
+
+// Without level order: item k's C ring (block n) on its tile T (if given)
+// and in memory (if to_mem), its foreign cells in Fs already: one pass over
+// the plan entries (stored by class: copies, fine-to-coarse, coarse-to-fine,
+// so that a warp mostly takes one kind). Ends with a barrier.
+template <int N>
+__device__ void fast_ring_c(const DevState& s, const Geo<N>& G, int k, int w, const ItemRec& r,
+                            const double* Fs, double* T, bool to_mem) {
+    const int R = (w == 2) ? ring2_len(G.nx, G.ny) : ring1_len(G.nx, G.ny);
+    const int* pl = ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)k * R * PLAN_INTS;
+    for (int e = threadIdx.x; e < r.na + r.n2 + r.n3; e += blockDim.x)
+        c_entry<N>(s, G, pl, R, e, r.n, w, Fs, T, to_mem);
+    __syncthreads();
+}
+
+// the same for the h/g ring on the staged planes As (if given): copies per
+// field, interpolated cells per population (both fields)
+template <int N>
+__device__ void fast_ring_hg(const DevState& s, const Geo<N>& G, int k, const ItemRec& r,
+                             const double* Fs, double* As, bool to_mem) {
+    const int RG = ring1_len(G.nx, G.ny);
+    const int* pl = s.plan_hg + (size_t)k * RG * PLAN_INTS;
+    const int nC = 2 * r.na, nI = r.n2 + r.n3;
+    for (int u = threadIdx.x; u < nC + 9 * nI; u += blockDim.x) {
+        if (u < nC) {
+            hg_copy<N>(s, G, pl, RG, u % r.na, u / r.na, r.n, As, to_mem);
+        } else {
+            const int v = u - nC;
+            hg_interp<N>(s, G, pl, RG, r.na + v % nI, v / nI, r.n, Fs, As, to_mem);
+        }
+    }
+    __syncthreads();
 }
 
 // C ghost fill of width w (Fill_Ghost_Cells_C.f90:2-416, Fill_Ghost_Cells_C2
@@ -1170,15 +1216,15 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
             [&](int k, int n, const NbInfo& nbi) {
                 foreign_c<N>(s, k, w, nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
                 if (nbi.wait[q]) {
-                    fill_ring_c<N>(s, G, k, n, w, 1, 0, Fs, nullptr);
+                    fill_ring_c<N>(s, G, k, n, w, 1, Fs);
                     wait_coarse(s, q, nbi);
-                    fill_ring_c<N>(s, G, k, n, w, 2, 0, Fs, nullptr);
+                    fill_ring_c<N>(s, G, k, n, w, 2, Fs);
                 } else {
-                    fill_ring_c<N>(s, G, k, n, w, 0, nbi.na[q] + nbi.nb[q], Fs, nullptr);
+                    fill_ring_c<N>(s, G, k, n, w, 0, Fs);
                 }
             },
             [&](int n, const NbInfo& nbi) { wall_c<N>(s, G, n, nbi, w); });
-    __shared__ int srec[2][6];  // without level order: records of the current and the next item
+    __shared__ int srec[2][REC_WORDS];  // without level order: records of this and the next item
     if (CONSUMER == CONS_NONE) {  // Fill_Ghost_Cells_C(2) alone: without level order, the rings in memory
         if (fast)
             for (int c = blockIdx.x; c < total; c += gridDim.x) {
@@ -1186,8 +1232,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
                 __syncthreads();
                 const ItemRec r = item_rec_of(srec[0]);
                 foreign_c<N>(s, c, w, r.nf, true, Fs);
-                fill_ring_c<N>(s, G, c, r.n, w, 0, r.na + r.nb, Fs, nullptr);
-                __syncthreads();
+                fast_ring_c<N>(s, G, c, w, r, Fs, nullptr, true);
                 if (r.w3 || r.w4) wall_c_rows<N>(s, G, r.n, w, r.w3, r.w4, nullptr);
                 __syncthreads();
             }
@@ -1247,8 +1292,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         phase ^= 1u << st;
         double* T = tiles + st * SD;
         if (fast) {  // the ring, then Symmetric_C(2)_3/4, on the tile (and in memory if wr)
-            fill_ring_c<N>(s, G, c, n, w, 0, r.na + r.nb, Fs, T, wr != 0);
-            __syncthreads();
+            fast_ring_c<N>(s, G, c, w, r, Fs, T, wr != 0);
             if (r.w3 || r.w4) {
                 wall_c_rows<N>(s, G, n, w, r.w3, r.w4, T, wr != 0);
                 __syncthreads();
@@ -1301,7 +1345,7 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
     unsigned phase = 0;
 
     if (fast) {
-        __shared__ int srec[2][6];  // records of the current and the next item
+        __shared__ int srec[2][REC_WORDS];  // records of the current and the next item
         int c = blockIdx.x, rb = 0;
         if (c < total) item_rec_stage(s, c, q, srec[0]);
         __syncthreads();
@@ -1318,8 +1362,7 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
             }
             phase ^= 1u;
             // the ring, then Bounce_Back_3/4, on the staged planes (and in memory if wr)
-            fill_ring_hg<N>(s, G, c, r.n, 0, r.na, r.nb, Fs, As, wr != 0);
-            __syncthreads();
+            fast_ring_hg<N>(s, G, c, r, Fs, As, wr != 0);
             if (r.w3 || r.w4) {
                 bounce_back_staged<N>(s, G, r.n, r.w3, r.w4, As, wr != 0);
                 __syncthreads();
@@ -1338,11 +1381,11 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
         [&](int k, int n, const NbInfo& nbi) {
             foreign_hg<N>(s, G, k, nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
             if (nbi.wait[q]) {
-                fill_ring_hg<N>(s, G, k, n, 1, 0, 0, Fs, nullptr);
+                fill_ring_hg<N>(s, G, k, n, 1, Fs);
                 wait_coarse(s, q, nbi);
-                fill_ring_hg<N>(s, G, k, n, 2, 0, 0, Fs, nullptr);
+                fill_ring_hg<N>(s, G, k, n, 2, Fs);
             } else {
-                fill_ring_hg<N>(s, G, k, n, 0, nbi.na[q], nbi.nb[q], Fs, nullptr);
+                fill_ring_hg<N>(s, G, k, n, 0, Fs);
             }
         },
         [&](int n, const NbInfo& nbi) { bounce_back<N>(s, G, n, nbi); });
@@ -1566,7 +1609,7 @@ void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t 
 
 void launch_build_plans(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
     cudaMemsetAsync(s.fillinfo, 0, NQUEUES * sizeof(int), st);
-#define C_(N) k_build_plans<N><<<lc.grid_leaves, 128, 9 * sizeof(int) * ring1_len(s.nx, s.ny), st>>>(s)
+#define C_(N) k_build_plans<N><<<lc.num_sms * 8, 128, 9 * sizeof(int) * ring1_len(s.nx, s.ny), st>>>(s)
     DISPATCH(s, C_);
 #undef C_
     count_launches(1);
