@@ -392,8 +392,8 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     if ((p->dx0 >> p->max_levels) < 1) return AMRLBM_ERR_ARG;  // dx stays an integer >= 1
     if (p->dx0 & (p->dx0 - 1)) return AMRLBM_ERR_ARG;  // powers of two (L0/nx = 2**maxLevels)
     {  // fill plans hold 31-bit offsets into the A pool and 31-bit plan indices
-        const size_t ap = ((size_t)p->nx + 5 + 3) / 4 * 4;
-        const size_t aplane = ((p->ny + 2) * ap + 15) / 16 * 16;
+        const size_t ap = (size_t)p->nx + 2;
+        const size_t aplane = (p->ny + 2) * ap;
         const size_t r2 = 4 * ((size_t)p->nx + p->ny) + 16;
         if (((size_t)p->max_blks + 1) * 9 * aplane >= (1ull << 31) ||
             ((size_t)p->max_blks + 1) * r2 >= (1ull << 31))
@@ -414,8 +414,8 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     s.ny = ny;
     s.max_blks = p->max_blks;
     s.fl_cap = p->max_blks / 4 + 2;
-    s.ap = (int)round_up(nx + 5, 4);
-    s.aplane = (int)round_up((size_t)(ny + 2) * s.ap, 16);
+    s.ap = nx + 2;                   // columns 0..nx+1 (nx even: rows and planes
+    s.aplane = (ny + 2) * s.ap;      // of 16-byte multiples)
     s.bplane = nx * ny;
     s.cp = (int)round_up(nx + 6, 4);
     s.cplane = (int)round_up((size_t)(ny + 4) * s.cp, 16);

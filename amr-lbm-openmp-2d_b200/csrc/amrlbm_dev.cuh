@@ -92,7 +92,7 @@ struct DevState {
 // ---------------------------------------------------------------------------
 // indexing
 __device__ __forceinline__ size_t a_idx(const DevState& s, int b, int q, int x, int y) {
-    return ((size_t)b * 9 + (q - 1)) * s.aplane + (size_t)y * s.ap + (x + 3);
+    return ((size_t)b * 9 + (q - 1)) * s.aplane + (size_t)y * s.ap + x;
 }
 __device__ __forceinline__ size_t b_idx(const DevState& s, int b, int q, int x, int y) {
     return ((size_t)b * 9 + (q - 1)) * s.bplane + (size_t)(y - 1) * s.nx + (x - 1);

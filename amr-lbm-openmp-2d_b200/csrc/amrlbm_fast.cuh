@@ -12,14 +12,14 @@ struct Geo {
     __device__ __forceinline__ explicit Geo(const DevState& s)
         : nx(N ? N : s.nx),
           ny(N ? N : s.ny),
-          ap(N ? ((N + 5 + 3) / 4) * 4 : s.ap),
-          aplane(N ? (((N + 2) * (((N + 5 + 3) / 4) * 4) + 15) / 16) * 16 : s.aplane),
+          ap(N ? N + 2 : s.ap),
+          aplane(N ? (N + 2) * (N + 2) : s.aplane),
           bplane(N ? N * N : s.bplane),
           cp(N ? ((N + 6 + 3) / 4) * 4 : s.cp),
           cplane(N ? (((N + 4) * (((N + 6 + 3) / 4) * 4) + 15) / 16) * 16 : s.cplane),
           pplane(N ? N * N : s.pplane) {}
     __device__ __forceinline__ size_t a(int b, int q, int x, int y) const {
-        return ((size_t)b * 9 + (q - 1)) * aplane + (size_t)(y * ap + (x + 3));
+        return ((size_t)b * 9 + (q - 1)) * aplane + (size_t)(y * ap + x);
     }
     __device__ __forceinline__ size_t bb(int b, int q, int x, int y) const {
         return ((size_t)b * 9 + (q - 1)) * bplane + (size_t)((y - 1) * nx + (x - 1));
