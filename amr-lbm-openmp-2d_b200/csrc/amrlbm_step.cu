@@ -587,30 +587,35 @@ __device__ __forceinline__ bool fast_fill(const DevState& s, int q) {
 // reference.
 __device__ __forceinline__ double foreign_value(const int* fb, int fmax, int j, const double* A,
                                                 size_t qo, bool live) {
-    if (!live) return ldcg(A + (unsigned)__ldg(fb + 10 * fmax + j) + qo);
-    const int meta = __ldg(fb + j);
-    if (plan_kind(meta) == 1) return __ldg(A + (unsigned)__ldg(fb + fmax + j) + qo);
+    if (!live) return ldcg(A + (unsigned)fb[10 * fmax + j] + qo);
+    const int meta = fb[j];
+    if (plan_kind(meta) == 1) return __ldg(A + (unsigned)fb[fmax + j] + qo);
     double g[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) g[i] = __ldg(A + (unsigned)__ldg(fb + (1 + i) * fmax + j) + qo);
+    for (int i = 0; i < 9; ++i) g[i] = __ldg(A + (unsigned)fb[(1 + i) * fmax + j] + qo);
     return plan_combine(meta, g);
 }
 
-// foreign cells of item k of a C fill (w: ring width) into Fs; ends with a
-// barrier when there are any (nf is block-uniform)
+// foreign cell records of item k of the C fills and of the h/g fill
+__device__ __forceinline__ const int* frn_c_of(const DevState& s, int k) {
+    return s.frn_c + (size_t)k * s.fmax * FRN_INTS;
+}
+__device__ __forceinline__ const int* frn_hg_of(const DevState& s, int k) {
+    return s.frn_hg + (size_t)k * s.fmax * FRN_INTS;
+}
+// foreign cells of a C fill (records fb, in memory or shared memory) into
+// Fs; ends with a barrier when there are any (nf is block-uniform)
 template <int N>
-__device__ void foreign_c(const DevState& s, int k, int w, int nf, bool live, double* Fs) {
+__device__ void foreign_c(const DevState& s, const int* fb, int nf, bool live, double* Fs) {
     if (nf == 0) return;
-    const int* fb = s.frn_c + (size_t)k * s.fmax * FRN_INTS;
     for (int j = threadIdx.x; j < nf; j += blockDim.x) Fs[j] = foreign_value(fb, s.fmax, j, s.C, 0, live);
     __syncthreads();
 }
 // the same for the h/g fill: one thread per (slot, field and population)
 template <int N>
-__device__ void foreign_hg(const DevState& s, const Geo<N>& G, int k, int nf, bool live,
+__device__ void foreign_hg(const DevState& s, const Geo<N>& G, const int* fb, int nf, bool live,
                            double* Fs) {
     if (nf == 0) return;
-    const int* fb = s.frn_hg + (size_t)k * s.fmax * FRN_INTS;
     for (int idx = threadIdx.x; idx < 18 * nf; idx += blockDim.x) {
         const int j = idx % nf, fq = idx / nf;
         Fs[fq * s.fmax + j] = foreign_value(fb, s.fmax, j, (fq >= 9) ? s.Ag : s.Ah,
@@ -632,7 +637,8 @@ __device__ __forceinline__ bool pass_takes(int mode, int kind) {
     return mode == 0 || ((kind == 3) == (mode == 2));
 }
 
-// One C ghost cell: plan entry e (plan array pl, ring length R, width w) of
+// One C ghost cell: plan entry e (plan words pl, in memory or shared memory;
+// ring length R, width w) of
 // block n, into memory (unless to_mem is false) and, if T is given, into the
 // block's shared C tile (index G.c(0,x,y)). Kind 1 and 2 sources are
 // interiors no launch of this fill writes; kind 3 sources are foreign slots
@@ -641,7 +647,7 @@ template <int N>
 __device__ __forceinline__ int c_entry(const DevState& s, const Geo<N>& G, const int* pl, int R,
                                        int e, int n, int w, const double* Fs, double* T,
                                        bool to_mem) {
-    const int meta = __ldg(pl + e);
+    const int meta = pl[e];
     const int kind = plan_kind(meta);
     if (kind == 0) return 0;
     int x, y;
@@ -655,16 +661,15 @@ __device__ __forceinline__ int c_entry(const DevState& s, const Geo<N>& G, const
     }
     double v;
     if (kind == 1) {
-        v = __ldg(s.C + (unsigned)__ldg(pl + R + e));
+        v = __ldg(s.C + (unsigned)pl[R + e]);
     } else {
         double g[9];
         if (kind == 2) {
 #pragma unroll
-            for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)__ldg(pl + (1 + i) * R + e));
+            for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)pl[(1 + i) * R + e]);
         } else {
 #pragma unroll
-            for (int i = 0; i < 9; ++i)
-                g[i] = c2f_source((unsigned)__ldg(pl + (1 + i) * R + e), Fs, s.C, 0);
+            for (int i = 0; i < 9; ++i) g[i] = c2f_source((unsigned)pl[(1 + i) * R + e], Fs, s.C, 0);
         }
         v = plan_combine(meta, g);
     }
@@ -691,7 +696,7 @@ __device__ void fill_ring_c(const DevState& s, const Geo<N>& G, int k, int n, in
 template <int N>
 __device__ __forceinline__ void hg_copy(const DevState& s, const Geo<N>& G, const int* pl, int RG,
                                         int e, int f, int n, double* As, bool to_mem) {
-    const int meta = __ldg(pl + e);
+    const int meta = pl[e];
     int x, y;
     ring1_xy(meta >> 8, G.nx, G.ny, x, y);
     if (plan_kind(meta) < 0) {
@@ -699,7 +704,7 @@ __device__ __forceinline__ void hg_copy(const DevState& s, const Geo<N>& G, cons
         return;
     }
     double* A = f ? s.Ag : s.Ah;
-    const double* src = A + (unsigned)__ldg(pl + RG + e);
+    const double* src = A + (unsigned)pl[RG + e];
     double v[9];
 #pragma unroll
     for (int qq = 0; qq < 9; ++qq) v[qq] = __ldg(src + (size_t)qq * G.aplane);
@@ -714,14 +719,14 @@ template <int N>
 __device__ __forceinline__ void hg_interp(const DevState& s, const Geo<N>& G, const int* pl, int RG,
                                           int e, int qq, int n, const double* Fs, double* As,
                                           bool to_mem) {
-    const int meta = __ldg(pl + e);
+    const int meta = pl[e];
     const int kind = plan_kind(meta);
     int x, y;
     ring1_xy(meta >> 8, G.nx, G.ny, x, y);
     const size_t qo = (size_t)qq * G.aplane;
     unsigned wd[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) wd[i] = (unsigned)__ldg(pl + (1 + i) * RG + e);
+    for (int i = 0; i < 9; ++i) wd[i] = (unsigned)pl[(1 + i) * RG + e];
 #pragma unroll
     for (int f = 0; f < 2; ++f) {
         double* A = f ? s.Ag : s.Ah;
@@ -1113,15 +1118,14 @@ __device__ __forceinline__ ItemRec item_rec_of(const int* w) {
     return o;
 }
 
-// Without level order: item k's C ring (block n) on its tile T (if given)
-// and in memory (if to_mem), its foreign cells in Fs already: one pass over
+// Without level order: an item's C ring (block r.n; plan words pl, ring
+// length R) on its tile T (if given) and in memory (if to_mem), its foreign
+// cells in Fs already: one pass over
 // the plan entries (stored by class: copies, fine-to-coarse, coarse-to-fine,
 // so that a warp mostly takes one kind). Ends with a barrier.
 template <int N>
-__device__ void fast_ring_c(const DevState& s, const Geo<N>& G, int k, int w, const ItemRec& r,
-                            const double* Fs, double* T, bool to_mem) {
-    const int R = (w == 2) ? ring2_len(G.nx, G.ny) : ring1_len(G.nx, G.ny);
-    const int* pl = ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)k * R * PLAN_INTS;
+__device__ void fast_ring_c(const DevState& s, const Geo<N>& G, const int* pl, int R, int w,
+                            const ItemRec& r, const double* Fs, double* T, bool to_mem) {
     for (int e = threadIdx.x; e < r.na + r.n2 + r.n3; e += blockDim.x)
         c_entry<N>(s, G, pl, R, e, r.n, w, Fs, T, to_mem);
     __syncthreads();
@@ -1130,10 +1134,9 @@ __device__ void fast_ring_c(const DevState& s, const Geo<N>& G, int k, int w, co
 // the same for the h/g ring on the staged planes As (if given): copies per
 // field, interpolated cells per population (both fields)
 template <int N>
-__device__ void fast_ring_hg(const DevState& s, const Geo<N>& G, int k, const ItemRec& r,
+__device__ void fast_ring_hg(const DevState& s, const Geo<N>& G, const int* pl, const ItemRec& r,
                              const double* Fs, double* As, bool to_mem) {
     const int RG = ring1_len(G.nx, G.ny);
-    const int* pl = s.plan_hg + (size_t)k * RG * PLAN_INTS;
     const int nC = 2 * r.na, nI = r.n2 + r.n3;
     for (int u = threadIdx.x; u < nC + 9 * nI; u += blockDim.x) {
         if (u < nC) {
@@ -1170,6 +1173,16 @@ __host__ __device__ inline size_t stage_doubles(int cplane, int bplane, int cons
     return (size_t)cplane + (stage_h(consumer) ? 9 * (size_t)bplane : 0) +
            (stage_g(consumer) ? 9 * (size_t)bplane : 0);
 }
+// ints of one staged item's plan words (R entries) and foreign records; a
+// multiple of 4 (16 bytes), as are both parts (R even, fmax a multiple of 4)
+__host__ __device__ inline int plan_stage_ints(int R, int fmax) {
+    return (PLAN_INTS * R + FRN_INTS * fmax + 3) & ~3;
+}
+// byte offset of a C fill's two staged plans: after the mbarriers, the two
+// stages of SD doubles and the foreign values
+__host__ __device__ inline size_t fill_c_plan_offset(size_t SD, int fmax) {
+    return (128 + 8 * (2 * SD + (size_t)fmax) + 15) & ~(size_t)15;
+}
 template <int N, int CONSUMER>
 __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     k_fill_c(DevState s, int w, int q, int wr) {
@@ -1186,6 +1199,12 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     double* Fs = tiles + 2 * SD;
     const size_t HP = 9 * (size_t)G.bplane;  // doubles of 9 planes
     const bool fast = fast_fill(s, q);
+    // without level order, stage st also holds its item's plan words and
+    // foreign records (plans + st * PS)
+    const int R = (w == 2) ? ring2_len(G.nx, G.ny) : ring1_len(G.nx, G.ny);
+    const int PS = plan_stage_ints(R, s.fmax);
+    int* plans = reinterpret_cast<int*>(smraw + fill_c_plan_offset(SD, s.fmax));
+    const unsigned plb = (unsigned)(PLAN_INTS * R) * 4, frb = (unsigned)(FRN_INTS * s.fmax) * 4;
     constexpr bool collide = (CONSUMER == CONS_COLLIDE_READ || CONSUMER == CONS_COLLIDE_FUSED);
     if (collide && blockIdx.x == 0 && t == 0)
         atomicAdd(&s.cnt->updates, (unsigned long long)total * (unsigned long long)(G.nx * G.ny));
@@ -1199,14 +1218,20 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
             collide_block<N, CONSUMER == CONS_COLLIDE_FUSED, true>(s, G, n, T, Hs, Gs);
     };
     const unsigned tb = (unsigned)G.cplane * 8, hb = (unsigned)HP * 8;
-    auto copy_tile = [&](int st, int nn) {  // thread 0
+    auto copy_tile = [&](int st, int nn, int c) {  // thread 0: item c, block nn
         double* T = tiles + st * SD;
         fence_proxy_async_all();
-        mbar_expect_tx(&bar[st], tb + (stage_h(CONSUMER) ? hb : 0) + (stage_g(CONSUMER) ? hb : 0));
+        mbar_expect_tx(&bar[st], tb + (stage_h(CONSUMER) ? hb : 0) + (stage_g(CONSUMER) ? hb : 0) +
+                                     (fast ? plb + frb : 0));
         bulk_g2s(T, s.C + (size_t)nn * G.cplane, tb, &bar[st]);
         if (stage_h(CONSUMER)) bulk_g2s(T + G.cplane, s.Bh + (size_t)nn * HP, hb, &bar[st]);
         if (stage_g(CONSUMER))
             bulk_g2s(T + G.cplane + (stage_h(CONSUMER) ? HP : 0), s.Bg + (size_t)nn * HP, hb, &bar[st]);
+        if (fast) {
+            int* P = plans + st * PS;
+            bulk_g2s(P, ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)c * R * PLAN_INTS, plb, &bar[st]);
+            bulk_g2s(P + PLAN_INTS * R, frn_c_of(s, c), frb, &bar[st]);
+        }
     };
 
     const int lmin = s.cnt->level_min;
@@ -1214,7 +1239,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         fill_phase(
             s, q, nbis, &s_next,
             [&](int k, int n, const NbInfo& nbi) {
-                foreign_c<N>(s, k, w, nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
+                foreign_c<N>(s, frn_c_of(s, k), nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
                 if (nbi.wait[q]) {
                     fill_ring_c<N>(s, G, k, n, w, 1, Fs);
                     wait_coarse(s, q, nbi);
@@ -1231,8 +1256,9 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
                 item_rec_stage(s, c, q, srec[0]);
                 __syncthreads();
                 const ItemRec r = item_rec_of(srec[0]);
-                foreign_c<N>(s, c, w, r.nf, true, Fs);
-                fast_ring_c<N>(s, G, c, w, r, Fs, nullptr, true);
+                foreign_c<N>(s, frn_c_of(s, c), r.nf, true, Fs);
+                fast_ring_c<N>(s, G, ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)c * R * PLAN_INTS,
+                               R, w, r, Fs, nullptr, true);
                 if (r.w3 || r.w4) wall_c_rows<N>(s, G, r.n, w, r.w3, r.w4, nullptr);
                 __syncthreads();
             }
@@ -1253,7 +1279,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         } else if (ld_acquire_i(flags + nn) == 0) {
             return false;
         }
-        copy_tile(st, nn);
+        copy_tile(st, nn, c);
         return true;
     };
     bool pend = false;  // thread 0: the next item's copy is still to start
@@ -1280,7 +1306,6 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
             r = item_rec_of(srec[st]);
             n = r.n;
             if ((int)cn < total) item_rec_stage(s, cn, q, srec[st ^ 1]);  // for the next item
-            foreign_c<N>(s, c, w, r.nf, true, Fs);                        // while the tile lands
         } else {
             n = __ldg(s.lvl_leaf + c);
         }
@@ -1292,7 +1317,9 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         phase ^= 1u << st;
         double* T = tiles + st * SD;
         if (fast) {  // the ring, then Symmetric_C(2)_3/4, on the tile (and in memory if wr)
-            fast_ring_c<N>(s, G, c, w, r, Fs, T, wr != 0);
+            const int* P = plans + st * PS;
+            foreign_c<N>(s, P + PLAN_INTS * R, r.nf, true, Fs);
+            fast_ring_c<N>(s, G, P, R, w, r, Fs, T, wr != 0);
             if (r.w3 || r.w4) {
                 wall_c_rows<N>(s, G, n, w, r.w3, r.w4, T, wr != 0);
                 __syncthreads();
@@ -1319,6 +1346,11 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
 // and streams; with level order the fill phase fills every leaf first and
 // consumer items come from a queue, their copy waiting for the block's flag.
 // Shared memory: mbarrier (128 bytes), h and g planes, the foreign values.
+// byte offset of the h/g fill's staged plan: after the mbarriers, the
+// h and g planes (FP doubles each) and the foreign values
+__host__ __device__ inline size_t hg_plan_offset(size_t FP, int fmax) {
+    return (128 + 8 * (2 * FP + 18 * (size_t)fmax) + 15) & ~(size_t)15;
+}
 template <int N>
 __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -1339,30 +1371,59 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
         bulk_g2s(As, s.Ah + (size_t)nn * FP, fb, bar);
         bulk_g2s(As + FP, s.Ag + (size_t)nn * FP, fb, bar);
     };
+    // without level order: plan words and foreign records of an item (Ps,
+    // mbarrier bar[1]), copied once the previous item's ring is filled
+    const int RG = ring1_len(G.nx, G.ny);
+    int* Ps = reinterpret_cast<int*>(smraw + hg_plan_offset(FP, s.fmax));
+    const unsigned plb = (unsigned)(PLAN_INTS * RG) * 4, frb = (unsigned)(FRN_INTS * s.fmax) * 4;
+    auto copy_plan = [&](int c) {  // thread 0
+        fence_proxy_async_all();
+        mbar_expect_tx(&bar[1], plb + frb);
+        bulk_g2s(Ps, s.plan_hg + (size_t)c * RG * PLAN_INTS, plb, &bar[1]);
+        bulk_g2s(Ps + PLAN_INTS * RG, frn_hg_of(s, c), frb, &bar[1]);
+    };
     const bool fast = fast_fill(s, q);
-    if (t == 0) mbar_init(bar, 1);
+    if (t == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+    }
     __syncthreads();
-    unsigned phase = 0;
+    unsigned phase = 0;  // bit b: parity of bar[b]'s next completion
 
     if (fast) {
         __shared__ int srec[2][REC_WORDS];  // records of the current and the next item
         int c = blockIdx.x, rb = 0;
-        if (c < total) item_rec_stage(s, c, q, srec[0]);
+        if (c < total) {
+            item_rec_stage(s, c, q, srec[0]);
+            if (t == 0) copy_plan(c);
+        }
         __syncthreads();
+        // bounded waits for the copies still in flight (bit b: bar[b]) before an exit
+        auto drain = [&](unsigned bits) {
+            for (int b = 0; b < 2; ++b)
+                if ((bits >> b) & 1u) mbar_wait(&bar[b], (phase >> b) & 1u);
+        };
         while (c < total) {
             const int cn = c + gridDim.x;
             const ItemRec r = item_rec_of(srec[rb]);
             if (t == 0) copy_planes(r.n);
             if (cn < total) item_rec_stage(s, cn, q, srec[rb ^ 1]);  // for the next iteration
-            foreign_hg<N>(s, G, c, r.nf, true, Fs);                  // while the planes land
-            if (__syncthreads_or(mbar_wait(bar, phase) ? 0 : 1)) {
+            if (__syncthreads_or(mbar_wait(&bar[1], (phase >> 1) & 1u) ? 0 : 1)) {
                 if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
-                mbar_wait(bar, phase);  // the copies must land before exit
+                drain(3u);
+                break;
+            }
+            phase ^= 2u;
+            foreign_hg<N>(s, G, Ps + PLAN_INTS * RG, r.nf, true, Fs);  // while the planes land
+            if (__syncthreads_or(mbar_wait(&bar[0], phase & 1u) ? 0 : 1)) {
+                if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
+                drain(1u);
                 break;
             }
             phase ^= 1u;
             // the ring, then Bounce_Back_3/4, on the staged planes (and in memory if wr)
-            fast_ring_hg<N>(s, G, c, r, Fs, As, wr != 0);
+            fast_ring_hg<N>(s, G, Ps, r, Fs, As, wr != 0);
+            if (t == 0 && cn < total) copy_plan(cn);  // the ring is filled: for the next iteration
             if (r.w3 || r.w4) {
                 bounce_back_staged<N>(s, G, r.n, r.w3, r.w4, As, wr != 0);
                 __syncthreads();
@@ -1379,7 +1440,7 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
     fill_phase(
         s, q, nbis, &s_next,
         [&](int k, int n, const NbInfo& nbi) {
-            foreign_hg<N>(s, G, k, nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
+            foreign_hg<N>(s, G, frn_hg_of(s, k), nbi.nf[q], nbi.lev[0] - 1 >= lmin, Fs);
             if (nbi.wait[q]) {
                 fill_ring_hg<N>(s, G, k, n, 1, Fs);
                 wait_coarse(s, q, nbi);
@@ -1401,9 +1462,9 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
             copy_planes(n);
             s_next = (int)cn;
         }
-        if (__syncthreads_or(mbar_wait(bar, phase) ? 0 : 1)) {
+        if (__syncthreads_or(mbar_wait(bar, phase & 1u) ? 0 : 1)) {
             if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
-            mbar_wait(bar, phase);
+            mbar_wait(bar, phase & 1u);
             break;
         }
         phase ^= 1u;
@@ -1552,14 +1613,16 @@ int queue_grid(K kernel, int nt, size_t smem, const LaunchCfg& lc) {
 }
 
 // shared memory of a C-fill launch: mbarriers, two stages, foreign values
-size_t fill_c_smem(const DevState& s, int consumer) {
-    return 128 + sizeof(double) * (2 * stage_doubles(s.cplane, s.bplane, consumer) + (size_t)s.fmax);
+size_t fill_c_smem(const DevState& s, int consumer, int width) {
+    const int R = (width == 2) ? ring2_len(s.nx, s.ny) : ring1_len(s.nx, s.ny);
+    return fill_c_plan_offset(stage_doubles(s.cplane, s.bplane, consumer), s.fmax) +
+           2 * sizeof(int) * (size_t)plan_stage_ints(R, s.fmax);
 }
 
 template <int N, int CONS>
 void fill_c_launch(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width, int q,
                    int wr) {
-    const size_t sm = fill_c_smem(s, CONS);
+    const size_t sm = fill_c_smem(s, CONS, width);
     const int nt = block_threads(s);
     smem_optin(k_fill_c<N, CONS>, sm);
     k_fill_c<N, CONS><<<queue_grid(k_fill_c<N, CONS>, nt, sm, lc), nt, sm, st>>>(s, width, q, wr);
@@ -1597,8 +1660,9 @@ void launch_fill_c(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int 
 
 void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int write_ring) {
     const int nt = block_threads(s);
-    // mbarrier, h and g planes, foreign values
-    const size_t sm = 128 + 18 * sizeof(double) * ((size_t)s.aplane + (size_t)s.fmax);
+    // mbarriers, h and g planes, foreign values, the staged plan
+    const size_t sm = hg_plan_offset(9 * (size_t)s.aplane, s.fmax) +
+                      sizeof(int) * (size_t)plan_stage_ints(ring1_len(s.nx, s.ny), s.fmax);
 #define C_(N)                                                                            \
     smem_optin(k_fill_hg_stream<N>, sm);                                                 \
     k_fill_hg_stream<N><<<queue_grid(k_fill_hg_stream<N>, nt, sm, lc), nt, sm, st>>>(s, write_ring)
