@@ -1093,18 +1093,27 @@ struct ItemRec {
     bool w3, w4;
 };
 constexpr int REC_WORDS = 7;
+// word t of an item record: n, nf, na, n2, n3, id[3] (bottom), id[4] (top)
+__device__ __forceinline__ const int* item_rec_word(const DevState& s, int c, int q, int t) {
+    const int off = t == 0   ? 0
+                    : t == 1 ? REC_NF + q
+                    : t == 2 ? REC_NA + q
+                    : t == 3 ? REC_N2 + q
+                    : t == 4 ? REC_N3 + q
+                             : t - 2;
+    return s.nbinfo + (size_t)c * NBI_STRIDE + off;
+}
 __device__ __forceinline__ void item_rec_stage(const DevState& s, int c, int q, int* dst) {
     const int t = threadIdx.x;
-    if (t < REC_WORDS) {
-        // n, nf, na, n2, n3, id[3] (bottom), id[4] (top)
-        const int off = t == 0   ? 0
-                        : t == 1 ? REC_NF + q
-                        : t == 2 ? REC_NA + q
-                        : t == 3 ? REC_N2 + q
-                        : t == 4 ? REC_N3 + q
-                                 : t - 2;
-        dst[t] = __ldg(s.nbinfo + (size_t)c * NBI_STRIDE + off);
-    }
+    if (t < REC_WORDS) dst[t] = __ldg(item_rec_word(s, c, q, t));
+}
+// the same without waiting for the loads: threads 0..6 gather the words with
+// cp.async and call cp_async_wait_all before the barrier that precedes the
+// first read of dst (thread 0, which copies word 0, may read it after its
+// own wait)
+__device__ __forceinline__ void item_rec_stage_async(const DevState& s, int c, int q, int* dst) {
+    const int t = threadIdx.x;
+    if (t < REC_WORDS) cp_async4(dst + t, item_rec_word(s, c, q, t));
 }
 __device__ __forceinline__ ItemRec item_rec_of(const int* w) {
     ItemRec o;
@@ -1249,7 +1258,9 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
                 }
             },
             [&](int n, const NbInfo& nbi) { wall_c<N>(s, G, n, nbi, w); });
-    __shared__ int srec[2][REC_WORDS];  // without level order: records of this and the next item
+    // without level order: records of this and the next item (srec[st]: the
+    // item of stage st)
+    __shared__ int srec[2][REC_WORDS];
     if (CONSUMER == CONS_NONE) {  // Fill_Ghost_Cells_C(2) alone: without level order, the rings in memory
         if (fast)
             for (int c = blockIdx.x; c < total; c += gridDim.x) {
@@ -1270,10 +1281,10 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     // thread 0: copy item c's C tile into stage st (with level order: once
     // its fill is done; without `block` only if it is done already; returns
     // whether the copy started)
-    auto start_tile = [&](int st, int c, bool block) {
-        const int nn = __ldg(s.lvl_leaf + c);
+    // (block nn; without level order the interior was written by the
+    // previous launch)
+    auto start_tile = [&](int st, int c, int nn, bool block) {
         if (fast) {
-            // the interior was written by the previous launch
         } else if (block) {
             if (!spin_flag(flags + nn)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
         } else if (ld_acquire_i(flags + nn) == 0) {
@@ -1288,7 +1299,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         mbar_init(&bar[1], 1);
         const int c0 = fast ? (int)blockIdx.x : (int)atomicAdd(&s.queue[4 * q + 1], 1u);
         s_next = c0;
-        if (c0 < total) start_tile(0, c0, true);
+        if (c0 < total) start_tile(0, c0, __ldg(s.lvl_leaf + c0), true);
     }
     if (fast && (int)blockIdx.x < total) item_rec_stage(s, blockIdx.x, q, srec[0]);
     __syncthreads();
@@ -1305,13 +1316,14 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         if (fast) {
             r = item_rec_of(srec[st]);
             n = r.n;
-            if ((int)cn < total) item_rec_stage(s, cn, q, srec[st ^ 1]);  // for the next item
+            if ((int)cn < total) item_rec_stage_async(s, cn, q, srec[st ^ 1]);  // for the next item
         } else {
             n = __ldg(s.lvl_leaf + c);
         }
         if (__syncthreads_or(mbar_wait(&bar[st], (phase >> st) & 1u) ? 0 : 1)) {
             if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
-            mbar_wait(&bar[st], (phase >> st) & 1u);  // the copy must land before exit
+            mbar_wait(&bar[st], (phase >> st) & 1u);  // the copies must land before exit
+            cp_async_wait_all();
             break;
         }
         phase ^= 1u << st;
@@ -1327,13 +1339,23 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         }
         if (t == 0) {
             s_next = (int)cn;
-            pend = ((int)cn < total) && !start_tile(st ^ 1, (int)cn, false);
+            int nn = 0;
+            if ((int)cn < total) {
+                if (fast) {
+                    cp_async_wait_all();  // word 0 of the next record, copied by this thread
+                    nn = srec[st ^ 1][0];
+                } else {
+                    nn = __ldg(s.lvl_leaf + cn);
+                }
+            }
+            pend = ((int)cn < total) && !start_tile(st ^ 1, (int)cn, nn, false);
         }
         consume(n, T);
+        if (fast) cp_async_wait_all();  // the next item's record
         __syncthreads();
         c = s_next;
         st ^= 1;
-        if (t == 0 && pend) start_tile(st, c, true);
+        if (t == 0 && pend) start_tile(st, c, __ldg(s.lvl_leaf + c), true);
     }
     if (!fast) queue_done(s, q);
 }
@@ -1402,12 +1424,13 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
         auto drain = [&](unsigned bits) {
             for (int b = 0; b < 2; ++b)
                 if ((bits >> b) & 1u) mbar_wait(&bar[b], (phase >> b) & 1u);
+            cp_async_wait_all();
         };
         while (c < total) {
             const int cn = c + gridDim.x;
             const ItemRec r = item_rec_of(srec[rb]);
             if (t == 0) copy_planes(r.n);
-            if (cn < total) item_rec_stage(s, cn, q, srec[rb ^ 1]);  // for the next iteration
+            if (cn < total) item_rec_stage_async(s, cn, q, srec[rb ^ 1]);  // for the next iteration
             if (__syncthreads_or(mbar_wait(&bar[1], (phase >> 1) & 1u) ? 0 : 1)) {
                 if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
                 drain(3u);
@@ -1429,6 +1452,7 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
                 __syncthreads();
             }
             stream_block<N>(s, G, r.n, As);
+            cp_async_wait_all();  // the next item's record
             __syncthreads();
             c = cn;
             rb ^= 1;
