@@ -1194,7 +1194,7 @@ __host__ __device__ inline size_t fill_c_plan_offset(size_t SD, int fmax) {
 }
 template <int N, int CONSUMER>
 __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
-    k_fill_c(DevState s, int w, int q, int wr) {
+    k_fill_c(const __grid_constant__ DevState s, int w, int q, int wr) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const Geo<N> G(s);
     __shared__ NbInfo nbis[2];
