@@ -54,8 +54,8 @@ enum { NBI_STRIDE = 64, PLAN_INTS = 10 };
 //            [blk][q][y][x], x,y = 1..nx,ny
 //   Ah, Ag : populations after collision with their ghost ring, the
 //            reference's Blk%h/g(:,0:nx+1,0:ny+1) between collision and
-//            streaming, [blk][q][y][col] with col = x+3 (x = 0..nx+1) so that
-//            interior rows start on 32-byte boundaries
+//            streaming, [blk][q][y][x], x,y = 0..nx+1,ny+1 (rows of nx+2:
+//            with nx, ny even, rows and planes are 16-byte multiples)
 //   C      : order parameter with both ghost rings, [blk][y+1][col],
 //            col = x+3 (x = -1..nx+2), y = -1..ny+2
 //   P,Ux,Uy: [blk][y][x], x,y = 1..nx,ny
