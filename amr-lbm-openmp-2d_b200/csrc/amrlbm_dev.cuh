@@ -37,7 +37,8 @@ struct Counters {
     int leaf_min, leaf_max;                      // level range of the current leaves
     int n_ref, n_der;                            // blocks refined / derefined by the last regrid
     int n_alloc_new;                             // refinements that appended new ids
-    int pad;
+    int n_ref_flag;    // blocks of the level range flagged for refinement by k_regrid_flags
+    int topo_changed;  // whether the last k_regrid_topo changed the mesh (plans rebuilt)
 };
 
 // Work queues of the level-ordered kernels (queue[4q..4q+2]: next fill item,

@@ -113,7 +113,8 @@ __device__ int block_scan(int flag, int* total) {
     return r;
 }
 
-// Stable compaction over ids 1..nb of pred(id) into out[base..]; returns count.
+// Stable compaction over ids 1..nb of pred(id) into out[base..] (out may be
+// null: count only); returns count.
 template <class Pred>
 __device__ int compact(int nb, int* out, int base, Pred pred) {
     int count = 0;
@@ -122,7 +123,7 @@ __device__ int compact(int nb, int* out, int base, Pred pred) {
         const int f = (id <= nb) ? (pred(id) ? 1 : 0) : 0;
         int tot;
         const int pos = block_scan(f, &tot);
-        if (f) out[base + count + pos] = id;
+        if (f && out) out[base + count + pos] = id;
         count += tot;
     }
     return count;
@@ -199,7 +200,14 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_flags(DevState s, 
         __syncthreads();
     }
     const int nd = compact(nb, s.der_list, 0, [&](int id) { return s.deref[id] != 0; });
-    if (threadIdx.x == 0) s.cnt->n_der = nd;
+    // blocks the refinement of k_regrid_topo will take (levels lmin..lmax)
+    const int nr = compact(nb, nullptr, 0, [&](int id) {
+        return s.refin[id] != 0 && s.level[id] >= lmin && s.level[id] <= lmax;
+    });
+    if (threadIdx.x == 0) {
+        s.cnt->n_der = nd;
+        s.cnt->n_ref_flag = nr;
+    }
 }
 
 // Restrict_Bilinear (Restrict.f90:14-65) for every block in der_list: the
@@ -325,6 +333,20 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_topo(DevState s, i
     const int nblks0 = cnt->nblks;
     const int lmin = lmin_o >= 0 ? lmin_o : cnt->level_min;
     const int lmax = lmax_o >= 0 ? lmax_o : cnt->level_max;
+    if (mode == 0 && cnt->n_der == 0 && cnt->n_ref_flag == 0) {
+        // nothing to refine or derefine: leaves, neighbours, work order and
+        // fill plans stay as they are
+        if (threadIdx.x == 0) {
+            cnt->n_ref = 0;
+            cnt->n_alloc_new = 0;
+            cnt->topo_changed = 0;
+            if (set_levels) {
+                cnt->level_min = cnt->leaf_min;
+                cnt->level_max = cnt->leaf_max;
+            }
+        }
+        return;
+    }
     if (mode != 2) {
         // ---- Derefine: Remove_Children for every listed parent (ascending ids)
         const int nd = (mode == 0) ? cnt->n_der : 0;
@@ -465,6 +487,8 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_topo(DevState s, i
     __syncthreads();
     for (int m = threadIdx.x; m < nleaf; m += blockDim.x) s.lvl_leaf[m] = s.leaf[s.lvl_leaf[m] - 1];
     if (threadIdx.x == 0) {
+        cnt->topo_changed = 1;  // k_build_plans rebuilds the plans and fill flags
+        for (int q = 0; q < NQUEUES; ++q) s.fillinfo[q] = 0;
         s.lvl_off[AMR_MAXLV] = nleaf;
         cnt->nleaf = nleaf;
         cnt->leaf_min = lo;

@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(128, 8) k_build_plans(DevState s) {
     __shared__ NbInfo cnb[9];     // coarser neighbours' records
     __shared__ int nfs;
     __shared__ int cls_n[2][4], cls_f[2][4];  // [C2 | ring-1 plans][class]: count, fill
+    if (!s.cnt->topo_changed) return;  // the mesh did not change: the plans stand
     const int nx = G.nx, ny = G.ny, R2 = ring2_len(nx, ny), R1 = ring1_len(nx, ny);
     const int total = s.lvl_off[AMR_MAXLV];
     const int t = threadIdx.x, fmax = s.fmax;
@@ -1696,7 +1697,6 @@ void launch_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t 
 }
 
 void launch_build_plans(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
-    cudaMemsetAsync(s.fillinfo, 0, NQUEUES * sizeof(int), st);
 #define C_(N) k_build_plans<N><<<lc.num_sms * 8, 128, 9 * sizeof(int) * ring1_len(s.nx, s.ny), st>>>(s)
     DISPATCH(s, C_);
 #undef C_
