@@ -149,6 +149,12 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_flags(DevState s, 
                                                                     double deref_tol) {
     const int nb = s.cnt->nblks;
     const int lmin = s.cnt->level_min, lmax = s.cnt->level_max;
+    // levels that hold a block flagged for refinement / derefinement: the
+    // closure passes of the other levels have nothing to do (each pass only
+    // adds flags one level down, after the barrier that ends the pass before)
+    __shared__ unsigned s_rmask, s_dmask;
+    if (threadIdx.x == 0) s_rmask = s_dmask = 0u;
+    __syncthreads();
     for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
         uint8_t r = 0;
         if (s.is_leaf[n]) {
@@ -158,16 +164,21 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_flags(DevState s, 
                 r = 1;
         }
         s.refin[n] = r;
+        if (r) atomicOr(&s_rmask, 1u << s.level[n]);
     }
     __syncthreads();
     // closure: a refining block's coarser (Level-1) leaf neighbours refine too;
     // processed from fine to coarse, every propagation goes one level down
     for (int L = s.max_levels; L >= 1; --L) {
+        if (!((s_rmask >> L) & 1u)) continue;
         for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
             if (s.level[n] != L || !s.refin[n]) continue;
             for (int I = 1; I <= 8; ++I) {
                 const int b = resolve_chk(s, n, I);
-                if (b > 0 && s.level[b] == L - 1 && s.is_leaf[b]) s.refin[b] = 1;
+                if (b > 0 && s.level[b] == L - 1 && s.is_leaf[b]) {
+                    s.refin[b] = 1;
+                    atomicOr(&s_rmask, 1u << (L - 1));
+                }
             }
         }
         __syncthreads();
@@ -186,9 +197,11 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_flags(DevState s, 
             }
         }
         s.deref[n] = d;
+        if (d) atomicOr(&s_dmask, 1u << s.level[n]);
     }
     __syncthreads();
     for (int L = lmax - 1; L >= lmin - 1; --L) {
+        if (L < 0 || !((s_dmask >> L) & 1u)) continue;
         for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
             if (s.level[n] != L || !s.deref[n]) continue;
             const bool ok = deref_ok(s, n, 1, 2, 4) && deref_ok(s, n, 2, 1, 3) &&

@@ -1409,17 +1409,18 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
     if (t == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
+        // without level order the first item's plan and planes are copied at once
+        if (fast && (int)blockIdx.x < total) {
+            copy_plan(blockIdx.x);
+            copy_planes(__ldg(s.lvl_leaf + blockIdx.x));
+        }
     }
-    __syncthreads();
     unsigned phase = 0;  // bit b: parity of bar[b]'s next completion
 
     if (fast) {
         __shared__ int srec[2][REC_WORDS];  // records of the current and the next item
         int c = blockIdx.x, rb = 0;
-        if (c < total) {
-            item_rec_stage(s, c, q, srec[0]);
-            if (t == 0) copy_plan(c);
-        }
+        if (c < total) item_rec_stage(s, c, q, srec[0]);
         __syncthreads();
         // bounded waits for the copies still in flight (bit b: bar[b]) before an exit
         auto drain = [&](unsigned bits) {
@@ -1430,7 +1431,7 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
         while (c < total) {
             const int cn = c + gridDim.x;
             const ItemRec r = item_rec_of(srec[rb]);
-            if (t == 0) copy_planes(r.n);
+            if (t == 0 && c != (int)blockIdx.x) copy_planes(r.n);
             if (cn < total) item_rec_stage_async(s, cn, q, srec[rb ^ 1]);  // for the next iteration
             if (__syncthreads_or(mbar_wait(&bar[1], (phase >> 1) & 1u) ? 0 : 1)) {
                 if (t == 0) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 100 + q);
@@ -1461,6 +1462,7 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
         return;
     }
 
+    __syncthreads();  // the mbarriers are initialised
     const int lmin = s.cnt->level_min;
     fill_phase(
         s, q, nbis, &s_next,
