@@ -250,3 +250,33 @@ def test_level_range_narrower_than_the_leaves(case, narrow):
             orc.macroscopic_values_g()
             gpu.macroscopic_values_g()
             compare_state(gpu, orc)
+
+
+@pytest.mark.parametrize("case", ["reference_default", "tiny_minlevels0", "small_16x16"])
+@pytest.mark.parametrize("narrow", ["finest_out", "coarsest_out"])
+def test_regrid_with_a_narrower_level_range(case, narrow):
+    """Refine_Derefine_Mesh with LevelMin..LevelMax narrower than the leaves:
+    flags outside the range refine nothing (Refine.f90's DO L = LevelMin,
+    LevelMax), so a regrid whose only flags lie outside it changes nothing
+    and keeps the fill plans; then the fused loop goes on from there."""
+    p = CASES[case]()
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    with AmrLbm(p) as gpu:
+        gpu.initialize_rising_bubble()
+        for step in range(3):
+            lo, hi = orc.determine_min_max_levels()
+            assert gpu.determine_min_max_levels() == (lo, hi)
+            if hi > lo:
+                a, b = (lo, hi - 1) if narrow == "finest_out" else (lo + 1, hi)
+                orc.set_level_range(a, b)
+                gpu.set_level_range(a, b)
+            orc.macroscopic_values_g()
+            gpu.macroscopic_values_g()
+            orc.refine_derefine_mesh()
+            gpu.refine_derefine_mesh()
+            compare_state(gpu, orc)
+        orc.main_loop(4)
+        gpu.main_loop(4)
+        gpu.sync()
+        compare_state(gpu, orc)
