@@ -650,70 +650,90 @@ __global__ void k_minmax(DevState s) {
 // Output (AMR_Rising_2D_OMP.f90:456-489) with a fixed summation order: per
 // leaf block in (j,i) order, then over blocks in leaf-list order. out[8] =
 // non-finite flag. part: 8 doubles per leaf (scratch, >= 8*nleaf).
+// one CTA per leaf: the block's C and Uy staged in shared memory (coalesced),
+// then thread 0 forms the block's sums in (j, i) order from there
 __global__ void k_diag_blocks(DevState s, double* part) {
-    const int nleaf = s.cnt->nleaf, nx = s.nx, ny = s.ny;
-    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < nleaf; m += gridDim.x * blockDim.x) {
+    extern __shared__ double sh[];  // [C | Uy] of one block, (j-1)*nx + (i-1)
+    const int nleaf = s.cnt->nleaf, nx = s.nx, ny = s.ny, nc = nx * ny;
+    for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
         const int n = s.leaf[m];
-        const int dx = s.dx[n];
-        const double a = (double)(dx * dx);
-        const PhysD& ph = s.ph;
-        double mass = 0, rmin = 10, rmax = -10, umax = 0, vol = 0, ysum = 0, vsum = 0, phase = 0;
-        bool finite = true;
-        for (int j = 1; j <= ny; ++j)
-            for (int i = 1; i <= nx; ++i) {
-                const double C = s.C[c_idx(s, n, i, j)];
-                const double Rho = ph.Rhol + C * (ph.Rhoh - ph.Rhol);
-                rmin = fmin(rmin, Rho);
-                rmax = fmax(rmax, Rho);
-                mass = mass + Rho * a;
-                const double uy = s.Uy[p_idx(s, n, i, j)];
-                umax = fmax(umax, fabs(uy));
-                const double yc = (double)(s.bj[n] * dx * ny) + dx * (j - 0.5);
-                const double wgt = (1.0 - C) * a;
-                vol = vol + wgt;
-                ysum = ysum + wgt * yc;
-                vsum = vsum + wgt * uy;
-                phase = phase + C * a;
-                if (!isfinite(C) || !isfinite(uy)) finite = false;
-            }
-        double* o = part + 9 * (size_t)m;
-        o[0] = mass;
-        o[1] = rmin;
-        o[2] = rmax;
-        o[3] = umax;
-        o[4] = vol;
-        o[5] = ysum;
-        o[6] = vsum;
-        o[7] = phase;
-        o[8] = finite ? 0.0 : 1.0;
+        for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+            const int i = c % nx + 1, j = c / nx + 1;
+            sh[c] = s.C[c_idx(s, n, i, j)];
+            sh[nc + c] = s.Uy[p_idx(s, n, i, j)];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int dx = s.dx[n];
+            const double a = (double)(dx * dx);
+            const PhysD& ph = s.ph;
+            double mass = 0, rmin = 10, rmax = -10, umax = 0, vol = 0, ysum = 0, vsum = 0, phase = 0;
+            bool finite = true;
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) {
+                    const double C = sh[(j - 1) * nx + (i - 1)];
+                    const double Rho = ph.Rhol + C * (ph.Rhoh - ph.Rhol);
+                    rmin = fmin(rmin, Rho);
+                    rmax = fmax(rmax, Rho);
+                    mass = mass + Rho * a;
+                    const double uy = sh[nc + (j - 1) * nx + (i - 1)];
+                    umax = fmax(umax, fabs(uy));
+                    const double yc = (double)(s.bj[n] * dx * ny) + dx * (j - 0.5);
+                    const double wgt = (1.0 - C) * a;
+                    vol = vol + wgt;
+                    ysum = ysum + wgt * yc;
+                    vsum = vsum + wgt * uy;
+                    phase = phase + C * a;
+                    if (!isfinite(C) || !isfinite(uy)) finite = false;
+                }
+            double* o = part + 9 * (size_t)m;
+            o[0] = mass;
+            o[1] = rmin;
+            o[2] = rmax;
+            o[3] = umax;
+            o[4] = vol;
+            o[5] = ysum;
+            o[6] = vsum;
+            o[7] = phase;
+            o[8] = finite ? 0.0 : 1.0;
+        }
+        __syncthreads();
     }
 }
 
+// the per-block partials combined in leaf-list order: chunks of DIAG_CHUNK
+// leaves staged in shared memory by all threads, thread k < 9 running
+// quantity k's sum (or min / max) through them in order
+#define DIAG_CHUNK 512
 __global__ void k_diag_final(DevState s, const double* part, double* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const int nleaf = s.cnt->nleaf;
-    double mass = 0, rmin = 10, rmax = -10, umax = 0, vol = 0, ysum = 0, vsum = 0, phase = 0, bad = 0;
-    for (int m = 0; m < nleaf; ++m) {
-        const double* o = part + 9 * (size_t)m;
-        mass = mass + o[0];
-        rmin = fmin(rmin, o[1]);
-        rmax = fmax(rmax, o[2]);
-        umax = fmax(umax, o[3]);
-        vol = vol + o[4];
-        ysum = ysum + o[5];
-        vsum = vsum + o[6];
-        phase = phase + o[7];
-        bad = bad + o[8];
+    __shared__ double sh[9 * DIAG_CHUNK];
+    __shared__ double res[9];
+    const int nleaf = s.cnt->nleaf, t = threadIdx.x;
+    double acc = (t == 1) ? 10.0 : ((t == 2) ? -10.0 : 0.0);
+    for (int base = 0; base < nleaf; base += DIAG_CHUNK) {
+        const int cnt = min(DIAG_CHUNK, nleaf - base);
+        for (int u = t; u < 9 * cnt; u += blockDim.x) sh[u] = part[9 * (size_t)base + u];
+        __syncthreads();
+        if (t < 9)
+            for (int m = 0; m < cnt; ++m) {
+                const double v = sh[9 * m + t];
+                acc = (t == 1) ? fmin(acc, v) : ((t == 2 || t == 3) ? fmax(acc, v) : acc + v);
+            }
+        __syncthreads();
     }
-    out[0] = mass;
-    out[1] = rmin;
-    out[2] = rmax;
-    out[3] = umax;
-    out[4] = vol;
-    out[5] = ysum / vol;
-    out[6] = vsum / vol;
-    out[7] = phase;
-    out[8] = bad;
+    if (t < 9) res[t] = acc;
+    __syncthreads();
+    if (t == 0) {
+        out[0] = res[0];
+        out[1] = res[1];
+        out[2] = res[2];
+        out[3] = res[3];
+        out[4] = res[4];
+        out[5] = res[5] / res[4];
+        out[6] = res[6] / res[4];
+        out[7] = res[7];
+        out[8] = res[8];
+    }
 }
 
 size_t tile_bytes(const DevState& s) { return (size_t)(s.nx + 4) * (s.ny + 4) * sizeof(double); }
@@ -784,7 +804,7 @@ void launch_flag_level(const DevState& s, cudaStream_t st, int level) {
 void launch_diag(const DevState& s, cudaStream_t st, double* out9) {
     // out9: device buffer of 9 + 9*max_blks doubles
     double* part = out9 + 9;
-    k_diag_blocks<<<64, 128, 0, st>>>(s, part);
-    k_diag_final<<<1, 32, 0, st>>>(s, part, out9);
+    k_diag_blocks<<<1184, 128, 2 * sizeof(double) * (size_t)s.nx * s.ny, st>>>(s, part);
+    k_diag_final<<<1, 256, 0, st>>>(s, part, out9);
     count_launches(2);
 }
