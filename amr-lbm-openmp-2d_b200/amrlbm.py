@@ -36,6 +36,8 @@ ERR_NAN = 5
 ERR_DANGLING = 6
 ERR_STATE = 7
 ERR_TIMEOUT = 8
+ERR_CAPACITY = 9
+ERR_IO = 10
 
 F_LEAF, F_HASLEAF, F_REFIN, F_DEREF, F_ALLOC = 1, 2, 4, 8, 16
 
@@ -192,6 +194,7 @@ def load_library(path: str | None = None):
         "amrlbm_step": (ct.c_int, [vp, ct.c_int32]),
         "amrlbm_sync": (ct.c_int, [vp]),
         "amrlbm_diag": (ct.c_int, [vp, dp]),
+        "amrlbm_write_tecplot": (ct.c_int, [vp, ct.c_char_p, ct.c_int32]),
         "amrlbm_timer_start": (ct.c_int, [vp]),
         "amrlbm_timer_stop": (ct.c_int, [vp, ct.POINTER(ct.c_float)]),
         "amrlbm_profile_enable": (ct.c_int, [vp, ct.c_int32]),
@@ -326,6 +329,12 @@ class AmrLbm:
 
     def sync(self):
         self._check(self.lib.amrlbm_sync(self.ctx))
+
+    def tecplot_cell_center(self, path, t: int):
+        """TecPlot_CellCenter (TecPlot_ASCII.f90:2-86): the leaves as one
+        FE-quadrilateral zone in the reference's ASCII layout, written to
+        `path`; t is the time step T of the zone title."""
+        self._check(self.lib.amrlbm_write_tecplot(self.ctx, os.fsencode(path), int(t)))
 
     def output(self):
         """Output (AMR_Rising_2D_OMP.f90:456-489) + bubble centroid/rise velocity."""

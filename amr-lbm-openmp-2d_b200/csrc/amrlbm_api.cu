@@ -979,6 +979,34 @@ int amrlbm_diag(amrlbm_ctx* ctx, double out[8]) {
     return AMRLBM_OK;
 }
 
+int amrlbm_write_tecplot(amrlbm_ctx* ctx, const char* path, int32_t t) {
+    if (!ctx || !path) return AMRLBM_ERR_ARG;
+    if (int r = sync_check(ctx)) return r;
+    const Counters c = read_counters(ctx);
+    const int nx = ctx->prm.nx, ny = ctx->prm.ny, nl = c.nleaf;
+    const size_t Nn = (size_t)nl * (nx + 1) * (ny + 1), Ne = (size_t)nl * nx * ny;
+    // staging: node C (Nn), cell Ux, Uy, P (3 Ne), node X, Y (2 Nn ints)
+    if (int r = ensure_stage(ctx, Nn + 3 * Ne + Nn + 1, 0)) return r;
+    double* node_c = ctx->d_stage;
+    double* cell = node_c + Nn;
+    int* node_xy = reinterpret_cast<int*>(cell + 3 * Ne);
+    const double D = 2.0 * ctx->prm.radius;
+    std::vector<double> hc(Nn), hcell(3 * Ne);
+    std::vector<int> hxy(2 * Nn);
+    if (nl > 0) {
+        launch_tecplot(ctx->s, ctx->st, ctx->lc.num_sms, node_c, node_xy, cell, D, ctx->s.ph.Sigma);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hc.data(), node_c, Nn * 8, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(hcell.data(), cell, 3 * Ne * 8, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(hxy.data(), node_xy, 2 * Nn * 4, cudaMemcpyDeviceToHost, ctx->st));
+        if (int r = sync_check(ctx)) return r;
+    }
+    const double tv = (double)t * std::sqrt(ctx->s.ph.Gy / D);  // T*DSQRT(Gy/D)
+    if (tecplot_write(path, nx, ny, nl, ctx->prm.dx0 * nx, tv, hc.data(), hxy.data(), hcell.data()))
+        return fail(ctx, AMRLBM_ERR_IO, std::string("cannot write ") + path);
+    return AMRLBM_OK;
+}
+
 int amrlbm_timer_start(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
     CK(cudaEventRecord(ctx->t0, ctx->st));

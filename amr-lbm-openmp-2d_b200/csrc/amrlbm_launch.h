@@ -48,6 +48,12 @@ void launch_prolong(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_zero_children(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_flag_level(const DevState& s, cudaStream_t st, int level);
 void launch_diag(const DevState& s, cudaStream_t st, double* out8);
+// TecPlot_CellCenter: node and cell values of every leaf (amrlbm_tecplot.cu)
+void launch_tecplot(const DevState& s, cudaStream_t st, int num_sms, double* node_c, int* node_xy,
+                    double* cell, double D, double sigma);
+// writes the reference's ASCII file from those values; 0 on success
+int tecplot_write(const char* path, int nx, int ny, int nleaf, int L0, double t_value,
+                  const double* node_c, const int* node_xy, const double* cell);
 void launch_reset_queues(const DevState& s, cudaStream_t st);
 // number of kernels the launchers above issued (for the launch counter)
 long long launches_issued();

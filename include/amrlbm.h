@@ -52,7 +52,8 @@ enum {
     AMRLBM_ERR_DANGLING = 6,   /* neighbour pointer into a freed block's child array */
     AMRLBM_ERR_STATE = 7,      /* call out of order (e.g. step before init)    */
     AMRLBM_ERR_TIMEOUT = 8,    /* a bounded device wait ran out                */
-    AMRLBM_ERR_CAPACITY = 9    /* request larger than a fixed scratch area      */
+    AMRLBM_ERR_CAPACITY = 9,   /* request larger than a fixed scratch area      */
+    AMRLBM_ERR_IO = 10         /* an output file could not be written           */
 };
 
 /* flag bits of amrlbm_get_topology / amrlbm_set_topology */
@@ -202,6 +203,16 @@ int amrlbm_sync(amrlbm_ctx* ctx);
  *   out[7] phase volume sum C*dx^2
  * Returns AMRLBM_ERR_NAN if any leaf value is not finite. */
 int amrlbm_diag(amrlbm_ctx* ctx, double out[8]);
+
+/* TecPlot_CellCenter (TecPlot_ASCII.f90:2-86; call site
+ * AMR_Rising_2D_OMP.f90:308): the leaves as one FE-quadrilateral zone in the
+ * reference's ASCII layout, to `path` (the reference names its files
+ * Rising_Bubble_2D_<nn>.dat from a call counter; the caller chooses here).
+ * t: the time step T of the zone title T*sqrt(Gy/D), D = 2*radius. Node
+ * values of C need the ghost ring 1 of C, as the reference's do: call it
+ * between amrlbm_step calls (or after amrlbm_fill_ghost_c). Returns
+ * AMRLBM_ERR_IO if the file cannot be written. */
+int amrlbm_write_tecplot(amrlbm_ctx* ctx, const char* path, int32_t t);
 
 /* ---- timing (CUDA events on the context's stream) ----------------------- */
 int amrlbm_timer_start(amrlbm_ctx* ctx);
