@@ -1171,7 +1171,8 @@ __device__ void fast_ring_hg(const DevState& s, const Geo<N>& G, const int* pl, 
 // items are claimed from a queue, their tile copy waiting for the block's flag.
 // Shared memory: mbarriers (128 bytes), two stages (C tile and, for the
 // consumer, the block's post-streaming h and / or g planes), the foreign
-// values.
+// values, and without level order each stage's plan words and foreign
+// records (copied with the stage's tile).
 __host__ __device__ constexpr bool stage_h(int consumer) {
     return consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED;
 }
@@ -1368,7 +1369,11 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
 // item's ring on the staged planes (and in memory if wr), applies the walls
 // and streams; with level order the fill phase fills every leaf first and
 // consumer items come from a queue, their copy waiting for the block's flag.
-// Shared memory: mbarrier (128 bytes), h and g planes, the foreign values.
+// Shared memory: mbarriers (128 bytes), h and g planes, the foreign values,
+// and without level order one item's plan words and foreign records (copied
+// once the previous item's ring is filled; a CTA's first item has its plan
+// and planes copied at entry).
+
 // byte offset of the h/g fill's staged plan: after the mbarriers, the
 // h and g planes (FP doubles each) and the foreign values
 __host__ __device__ inline size_t hg_plan_offset(size_t FP, int fmax) {
