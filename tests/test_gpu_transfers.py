@@ -7,7 +7,8 @@ and writes of Blk(n)%h, %g, %C, %P, %Ux, %Uy (Parameters.f90:23-39).
 Round trips are bit for bit on ragged requests (none, one block, a reversed
 subset with gaps, every leaf); the batched and per-block entry points agree;
 fields left out of an upload keep their values; ids outside the pool are
-rejected with an error and change nothing."""
+rejected with an error and change nothing; a non-finite value uploaded into
+a leaf is reported by the diagnostics."""
 import numpy as np
 import pytest
 
@@ -110,3 +111,22 @@ def test_ids_outside_the_pool_are_rejected():
         after = sim.download_fields(ids)
         for k in FIELDS:
             assert np.array_equal(after[k], before[k]), k
+
+
+def test_non_finite_field_is_reported_by_the_diagnostics():
+    """Output (AMR_Rising_2D_OMP.f90:456-489) on a state with a NaN in C or
+    an infinite Uy in one leaf interior: AMRLBM_ERR_NAN instead of numbers;
+    a finite state again reports normally."""
+    with _started(steps=1) as sim:
+        sim.output()
+        bid = int(sim.leaves()[3])
+        b = sim.download_block(bid)
+        for field, bad in (("C", np.nan), ("Uy", np.inf)):
+            a = b[field].copy()
+            a[2, 2] = bad
+            sim.upload_block(bid, **{field: a})
+            with pytest.raises(AmrLbmError) as e:
+                sim.output()
+            assert e.value.status == amrlbm.ERR_NAN
+            sim.upload_block(bid, **{field: b[field]})
+            sim.output()
