@@ -1352,6 +1352,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
             }
             pend = ((int)cn < total) && !start_tile(st ^ 1, (int)cn, nn, false);
         }
+        __syncwarp();  // warp 0 reconverges after thread 0's copies, before the consumer work
         consume(n, T);
         if (fast) cp_async_wait_all();  // the next item's record
         __syncthreads();
