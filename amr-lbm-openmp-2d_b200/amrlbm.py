@@ -38,6 +38,7 @@ ERR_STATE = 7
 ERR_TIMEOUT = 8
 ERR_CAPACITY = 9
 ERR_IO = 10
+G_MRT, G_BGK = 0, 1  # collision models of g (amrlbm_set_g_collision)
 
 F_LEAF, F_HASLEAF, F_REFIN, F_DEREF, F_ALLOC = 1, 2, 4, 8, 16
 
@@ -166,6 +167,7 @@ def load_library(path: str | None = None):
         "amrlbm_create": (ct.c_int, [ct.POINTER(Params), ct.POINTER(vp)]),
         "amrlbm_destroy": (ct.c_int, [vp]),
         "amrlbm_set_physics": (ct.c_int, [vp, ct.POINTER(Physics)]),
+        "amrlbm_set_g_collision": (ct.c_int, [vp, ct.c_int32]),
         "amrlbm_last_error": (ct.c_char_p, [vp]),
         "amrlbm_device_bytes": (ct.c_int64, [vp]),
         "amrlbm_get_counts": (ct.c_int, [vp, i32p]),
@@ -293,6 +295,12 @@ class AmrLbm:
 
     def set_physics(self, phys: Physics):
         self._check(self.lib.amrlbm_set_physics(self.ctx, ct.byref(phys)))
+
+    def set_g_collision(self, model: int):
+        """G_MRT (MRT_Collision_AMR, the reference's) or G_BGK
+        (BGK_Collision_AMR, commented out in the reference at
+        LBM_Subroutines.f90:180)."""
+        self._check(self.lib.amrlbm_set_g_collision(self.ctx, int(model)))
 
     # -- Main_Loop call sites ---------------------------------------------
     def determine_min_max_levels(self):

@@ -421,6 +421,7 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     s.cplane = (int)round_up((size_t)(ny + 4) * s.cp, 16);
     s.pplane = nx * ny;
     s.min_levels = p->min_levels;
+    s.g_model = AMRLBM_G_MRT;
     s.max_levels = p->max_levels;
     amrlbm_physics ph;
     amrlbm_derive_physics(p, &ph);
@@ -524,12 +525,32 @@ int amrlbm_destroy(amrlbm_ctx* ctx) {
     return AMRLBM_OK;
 }
 
+// the captured intervals hold DevState by value and the kernel variants of
+// the settings they were captured with
+void drop_graphs(amrlbm_ctx* ctx) {
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    for (auto& kv : ctx->graphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        for (auto& pe : kv.second.prof) {
+            cudaEventDestroy(pe.second.first);
+            cudaEventDestroy(pe.second.second);
+        }
+    }
+    ctx->graphs.clear();
+    ctx->prof_pending = nullptr;
+}
+
 int amrlbm_set_physics(amrlbm_ctx* ctx, const amrlbm_physics* phys) {
     if (!ctx || !phys) return AMRLBM_ERR_ARG;
     ctx->s.ph = to_physd(*phys);
-    for (auto& kv : ctx->graphs)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    ctx->graphs.clear();  // kernels capture DevState by value
+    drop_graphs(ctx);
+    return AMRLBM_OK;
+}
+
+int amrlbm_set_g_collision(amrlbm_ctx* ctx, int32_t model) {
+    if (!ctx || (model != AMRLBM_G_MRT && model != AMRLBM_G_BGK)) return AMRLBM_ERR_ARG;
+    ctx->s.g_model = model;
+    drop_graphs(ctx);
     return AMRLBM_OK;
 }
 

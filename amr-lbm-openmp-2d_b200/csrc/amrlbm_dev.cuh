@@ -67,6 +67,7 @@ struct DevState {
     int cp, cplane;  // C row pitch and block stride
     int pplane;      // P/Ux/Uy block stride
     int min_levels, max_levels;
+    int g_model;     // collision of g: 0 MRT (the reference's), 1 BGK
     double *Ah, *Ag, *Bh, *Bg, *C, *P, *Ux, *Uy, *err;
     int *level, *dx, *bi, *bj, *parent, *child;  // child[4*id + k-1]
     int *nb_owner, *nb_slot, *nb_gen;            // [8*id + k-1] neighbour pointers

@@ -789,7 +789,10 @@ __device__ void wall_c(const DevState& s, const Geo<N>& G, int n, const NbInfo& 
 // launch. Writes the post-collision populations A to memory. FUSED: P, Ux,
 // Uy come from Macroscopic_Values_g_AMR (:205-240) evaluated here on the
 // same C ring.
-template <bool SAFE, bool FUSED, bool SH, int N>
+// BGK: the collision of g is BGK_Collision_AMR (LBM_Subroutines.f90:337-344,
+// g*(1-s9) + geq*s9) instead of MRT_Collision_AMR, the alternative the
+// reference leaves commented out at :180
+template <bool SAFE, bool FUSED, bool SH, int N, bool BGK = false>
 __device__ __forceinline__ unsigned collide_cell(const DevState& s, const Geo<N>& G, int n, int c,
                                                  double inv_dx, const double* T, const double* Hb,
                                                  const double* Gb) {
@@ -877,8 +880,16 @@ __device__ __forceinline__ unsigned collide_cell(const DevState& s, const Geo<N>
             const double Bk = ((double)d_ey(k) - Uy) * Gm * Fb;
             const double hc = Ak * (Ec(k) - ud_c) + Bk;
             const double geq = P * wk + dv.d3((Gm - wk) * Rho) - 0.5 * hc;
-            f[k] = ldp(Gn + (k - 1) * BP) - geq;
+            if (BGK)  // g(:)*(1.d0 - s9) + geq(:)*s9
+                f[k] = ldp(Gn + (k - 1) * BP) * (1.0 - s9) + geq * s9;
+            else
+                f[k] = ldp(Gn + (k - 1) * BP) - geq;
             hm[k] = Ak * (Em(k) - ud_m) + Bk;
+        }
+        if (BGK) {
+#pragma unroll
+            for (int k = 1; k <= 9; ++k) s.Ag[G.a(n, k, x, y)] = f[k] + hm[k];
+            return dv.bad;
         }
         // MRT_Collision_AMR (:348-361): Convert, relax 8 and 9, Reconvt, /36
         double m[10];
@@ -952,13 +963,13 @@ __device__ __forceinline__ unsigned macro_g_cell_f(const DevState& s, const Geo<
 // Collision of every cell of block n: the branch-free exact division path,
 // and the IEEE path for a cell whose flag says a quotient left its range.
 // SH: Hb and Gb point to shared memory (else to memory)
-template <int N, bool FUSED, bool SH>
+template <int N, bool FUSED, bool SH, bool BGK = false>
 __device__ __forceinline__ void collide_block(const DevState& s, const Geo<N>& G, int n,
                                               const double* T, const double* Hb, const double* Gb) {
     const double inv_dx = 1.0 / (double)__ldg(s.dx + n);  // dx is a power of two: exact
     for (int c = threadIdx.x; c < G.nx * G.ny; c += blockDim.x)
-        if (collide_cell<false, FUSED, SH>(s, G, n, c, inv_dx, T, Hb, Gb))
-            collide_cell<true, FUSED, SH>(s, G, n, c, inv_dx, T, Hb, Gb);
+        if (collide_cell<false, FUSED, SH, N, BGK>(s, G, n, c, inv_dx, T, Hb, Gb))
+            collide_cell<true, FUSED, SH, N, BGK>(s, G, n, c, inv_dx, T, Hb, Gb);
 }
 
 // Macroscopic_Values_g_AMR of every cell of block n; returns this thread's
@@ -1194,7 +1205,7 @@ __host__ __device__ inline int plan_stage_ints(int R, int fmax) {
 __host__ __device__ inline size_t fill_c_plan_offset(size_t SD, int fmax) {
     return (128 + 8 * (2 * SD + (size_t)fmax) + 15) & ~(size_t)15;
 }
-template <int N, int CONSUMER>
+template <int N, int CONSUMER, bool BGK = false>
 __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     k_fill_c(const __grid_constant__ DevState s, int w, int q, int wr) {
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -1226,7 +1237,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         if (CONSUMER == CONS_MACRO_G)
             err_reduce(s, n, macro_g_block<N, true>(s, G, n, T, Gs), red);
         else if (CONSUMER != CONS_NONE)
-            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED, true>(s, G, n, T, Hs, Gs);
+            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED, true, BGK>(s, G, n, T, Hs, Gs);
     };
     const unsigned tb = (unsigned)G.cplane * 8, hb = (unsigned)HP * 8;
     auto copy_tile = [&](int st, int nn, int c) {  // thread 0: item c, block nn
@@ -1518,7 +1529,7 @@ __device__ __forceinline__ void load_tile_c(const DevState& s, const Geo<N>& G, 
     __syncthreads();
 }
 
-template <int N>
+template <int N, bool BGK = false>
 __global__ void __launch_bounds__(256, 2) k_collide(DevState s) {
     extern __shared__ __align__(16) double T[];
     const Geo<N> G(s);
@@ -1528,8 +1539,8 @@ __global__ void __launch_bounds__(256, 2) k_collide(DevState s) {
     for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
         const int n = s.leaf[m];
         load_tile_c<N>(s, G, n, T);
-        collide_block<N, false, false>(s, G, n, T, s.Bh + (size_t)n * 9 * G.bplane,
-                                s.Bg + (size_t)n * 9 * G.bplane);
+        collide_block<N, false, false, BGK>(s, G, n, T, s.Bh + (size_t)n * 9 * G.bplane,
+                                            s.Bg + (size_t)n * 9 * G.bplane);
         __syncthreads();
     }
 }
@@ -1652,13 +1663,14 @@ size_t fill_c_smem(const DevState& s, int consumer, int width) {
            2 * sizeof(int) * (size_t)plan_stage_ints(R, s.fmax);
 }
 
-template <int N, int CONS>
+template <int N, int CONS, bool BGK = false>
 void fill_c_launch(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int width, int q,
                    int wr) {
     const size_t sm = fill_c_smem(s, CONS, width);
     const int nt = block_threads(s);
-    smem_optin(k_fill_c<N, CONS>, sm);
-    k_fill_c<N, CONS><<<queue_grid(k_fill_c<N, CONS>, nt, sm, lc), nt, sm, st>>>(s, width, q, wr);
+    smem_optin(k_fill_c<N, CONS, BGK>, sm);
+    k_fill_c<N, CONS, BGK><<<queue_grid(k_fill_c<N, CONS, BGK>, nt, sm, lc), nt, sm, st>>>(s, width, q,
+                                                                                         wr);
 }
 
 template <int N>
@@ -1666,8 +1678,18 @@ void fill_c_dispatch(const DevState& s, const LaunchCfg& lc, cudaStream_t st, in
                      int consumer, int q, int wr) {
     switch (consumer) {
         case CONS_NONE: fill_c_launch<N, CONS_NONE>(s, lc, st, width, q, wr); break;
-        case CONS_COLLIDE_READ: fill_c_launch<N, CONS_COLLIDE_READ>(s, lc, st, width, q, wr); break;
-        case CONS_COLLIDE_FUSED: fill_c_launch<N, CONS_COLLIDE_FUSED>(s, lc, st, width, q, wr); break;
+        case CONS_COLLIDE_READ:
+            if (s.g_model == 1)
+                fill_c_launch<N, CONS_COLLIDE_READ, true>(s, lc, st, width, q, wr);
+            else
+                fill_c_launch<N, CONS_COLLIDE_READ>(s, lc, st, width, q, wr);
+            break;
+        case CONS_COLLIDE_FUSED:
+            if (s.g_model == 1)
+                fill_c_launch<N, CONS_COLLIDE_FUSED, true>(s, lc, st, width, q, wr);
+            else
+                fill_c_launch<N, CONS_COLLIDE_FUSED>(s, lc, st, width, q, wr);
+            break;
         default: fill_c_launch<N, CONS_MACRO_G>(s, lc, st, width, q, wr); break;
     }
 }
@@ -1715,7 +1737,11 @@ void launch_collide(const DevState& s, const LaunchCfg& lc, cudaStream_t st) {
     const size_t sm = sizeof(double) * (size_t)s.cplane;
 #define C_(N)                      \
     smem_optin(k_collide<N>, sm); \
-    k_collide<N><<<lc.grid_leaves, block_threads(s), sm, st>>>(s)
+    smem_optin(k_collide<N, true>, sm); \
+    if (s.g_model == 1) \
+        k_collide<N, true><<<lc.grid_leaves, block_threads(s), sm, st>>>(s); \
+    else \
+        k_collide<N><<<lc.grid_leaves, block_threads(s), sm, st>>>(s)
     DISPATCH(s, C_);
 #undef C_
     count_launches(1);

@@ -106,6 +106,12 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out);
 int amrlbm_destroy(amrlbm_ctx* ctx);
 /* Replaces the derived constants (the Fortran driver computes its own). */
 int amrlbm_set_physics(amrlbm_ctx* ctx, const amrlbm_physics* phys);
+/* Collision model of g in Collision_h_g_AMR (LBM_Subroutines.f90:179-181):
+ * AMRLBM_G_MRT, MRT_Collision_AMR (:348-361), the reference's and the
+ * default; or AMRLBM_G_BGK, BGK_Collision_AMR (:337-344), the alternative
+ * the reference keeps commented out at :180. */
+enum { AMRLBM_G_MRT = 0, AMRLBM_G_BGK = 1 };
+int amrlbm_set_g_collision(amrlbm_ctx* ctx, int32_t model);
 const char* amrlbm_last_error(const amrlbm_ctx* ctx);
 /* Device memory held by the context, bytes. */
 int64_t amrlbm_device_bytes(const amrlbm_ctx* ctx);

@@ -92,6 +92,7 @@ struct orc_sim {
     long stepcount = 0;
     int err = 0;
     int level_jumps = 0;
+    int g_model = 0; /* collision of g: 0 MRT (the reference's), 1 BGK */
 
     /* field accessors in the reference's layouts */
     int NX2() const { return nx + 2; }
@@ -296,6 +297,12 @@ inline void mrt(double s9, const double* geq, double* g) {
     for (int i = 1; i <= 9; ++i) g[i] = g[i] - r[i];
 }
 
+/* BGK_Collision_AMR (LBM_Subroutines.f90:337-344), the alternative the
+ * reference leaves commented out at :180: g = g*(1 - s9) + geq*s9 */
+inline void bgk(double s9, const double* geq, double* g) {
+    for (int i = 1; i <= 9; ++i) g[i] = g[i] * (1.0 - s9) + geq[i] * s9;
+}
+
 /* Collision_h_g_AMR (LBM_Subroutines.f90:116-189) */
 void collision(const orc_sim& s, Block& b) {
     const Phys& ph = s.ph;
@@ -344,7 +351,10 @@ void collision(const orc_sim& s, Block& b) {
             const double s9 = 1.0 / tau;
             double gl[10];
             for (int k = 1; k <= 9; ++k) gl[k] = s.H(b.g, k, i, j);
-            mrt(s9, geq, gl);
+            if (s.g_model == 1)
+                bgk(s9, geq, gl);
+            else
+                mrt(s9, geq, gl);
             for (int k = 1; k <= 9; ++k) s.H(b.g, k, i, j) = gl[k] + hlp[k];
         }
 }
@@ -1577,6 +1587,13 @@ void orc_set_physics(orc_sim* s, const amrlbm_physics* o) {
     s->ph.Gy = o->gy;
     s->ph.M0 = o->m0;
     s->ph.wc = 1.0 / (0.5 + s->ph.M0 * 3.0);
+}
+
+/* the collision model of g (LBM_Subroutines.f90:179-181): 0 MRT, 1 BGK */
+int orc_set_g_collision(orc_sim* s, int model) {
+    if (model != 0 && model != 1) return 1;
+    s->g_model = model;
+    return 0;
 }
 
 /* AMR_LBM_Rising_Bubble start-up (AMR_Rising_2D_OMP.f90:49-67) */

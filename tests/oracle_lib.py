@@ -33,6 +33,7 @@ def lib():
             "orc_level_jump_count": (ct.c_int, [vp]),
             "orc_physics": (None, [vp, ct.POINTER(Physics)]),
             "orc_set_physics": (None, [vp, ct.POINTER(Physics)]),
+            "orc_set_g_collision": (ct.c_int, [vp, ct.c_int]),
             "orc_init_rising_bubble": (ct.c_int, [vp]),
             "orc_init_fields": (ct.c_int, [vp]),
             "orc_step": (ct.c_int, [vp, ct.c_int]),
@@ -110,6 +111,9 @@ class Oracle:
 
     def set_physics(self, ph):
         self.L.orc_set_physics(self.s, ct.byref(ph))
+
+    def set_g_collision(self, model):
+        assert self.L.orc_set_g_collision(self.s, model) == 0
 
     def initialize_rising_bubble(self):
         rc = self.L.orc_init_rising_bubble(self.s)

@@ -300,3 +300,44 @@ def test_regrid_with_a_narrower_level_range(case, narrow):
         gpu.main_loop(4)
         gpu.sync()
         compare_state(gpu, orc)
+
+
+@pytest.mark.parametrize("case,regrid_every,nsteps", [
+    ("tiny_minlevels0", 1, 8),
+    ("small_16x16", 3, 7),
+])
+def test_bgk_collision_option(case, regrid_every, nsteps):
+    """BGK_Collision_AMR (LBM_Subroutines.f90:337-344), which the reference
+    keeps commented out at :180, in place of MRT_Collision_AMR: phase by phase
+    and in the fused loop, bit for bit with the oracle under the same option;
+    switching the model between calls drops the captured intervals."""
+    p = CASES[case]()
+    p.regrid_every = regrid_every
+    orc = Oracle(p)
+    orc.set_g_collision(amrlbm.G_BGK)
+    orc.initialize_rising_bubble()
+    with AmrLbm(p) as gpu:
+        gpu.set_g_collision(amrlbm.G_BGK)
+        gpu.initialize_rising_bubble()
+        orc.fill_ghost_cells_c2()
+        gpu.fill_ghost_cells_c2()
+        orc.phase_field_lbm_h_g()
+        gpu.phase_field_lbm_h_g()
+        compare_fields(gpu, orc, fields=("h", "g"))
+        orc.macroscopic_values_h()
+        gpu.macroscopic_values_h()
+        orc.fill_ghost_cells_c()
+        gpu.fill_ghost_cells_c()
+        orc.macroscopic_values_g()
+        gpu.macroscopic_values_g()
+        orc.main_loop(nsteps)
+        gpu.main_loop(nsteps)
+        gpu.sync()
+        compare_state(gpu, orc)
+        for model in (amrlbm.G_MRT, amrlbm.G_BGK):
+            orc.set_g_collision(model)
+            gpu.set_g_collision(model)
+            orc.main_loop(3)
+            gpu.main_loop(3)
+            gpu.sync()
+            compare_state(gpu, orc)

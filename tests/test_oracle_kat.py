@@ -245,3 +245,24 @@ def test_oracle_matches_golden_fixtures(name):
         assert snapshot(o, p) == want["after_steps"]
     finally:
         o.close()
+
+
+def test_bgk_option_changes_g_only_through_the_collision():
+    """The oracle's BGK_Collision_AMR switch (LBM_Subroutines.f90:180): one
+    collide-fill-stream pass from the same start-up state leaves h equal
+    (the collision of h does not depend on the model of g) and changes g."""
+    import numpy as np
+    import amrlbm
+    from oracle_lib import Oracle
+    p = amrlbm.reference_params()
+    runs = []
+    for model in (amrlbm.G_MRT, amrlbm.G_BGK):
+        o = Oracle(p)
+        o.set_g_collision(model)
+        o.initialize_rising_bubble()
+        o.fill_ghost_cells_c2()
+        o.phase_field_lbm_h_g()
+        runs.append({int(b): o.download_block(int(b)) for b in o.leaves()})
+    same_h = all(np.array_equal(runs[0][b]["h"], runs[1][b]["h"]) for b in runs[0])
+    diff_g = any(not np.array_equal(runs[0][b]["g"], runs[1][b]["g"]) for b in runs[0])
+    assert same_h and diff_g
