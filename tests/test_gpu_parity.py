@@ -341,3 +341,29 @@ def test_bgk_collision_option(case, regrid_every, nsteps):
             gpu.main_loop(3)
             gpu.sync()
             compare_state(gpu, orc)
+
+
+def test_physics_replaced_between_calls():
+    """amrlbm_set_physics (a driver with its own Set_Rising_Bubble_Parameters,
+    AMR_Rising_2D_OMP.f90:235-263) between fused calls: the captured
+    intervals are rebuilt with the new constants, bit for bit with the oracle."""
+    p = tiny_params()
+    p.regrid_every = 2
+    orc = Oracle(p)
+    orc.initialize_rising_bubble()
+    with AmrLbm(p) as gpu:
+        gpu.initialize_rising_bubble()
+        orc.main_loop(3)
+        gpu.main_loop(3)
+        ph = orc.physics()
+        ph.tau_h = ph.tau_h * 1.5
+        ph.sigma = ph.sigma * 0.8
+        ph.beta = ph.beta * 0.8
+        ph.kappa = ph.kappa * 0.8
+        ph.gy = ph.gy * 2.0
+        orc.set_physics(ph)
+        gpu.set_physics(ph)
+        orc.main_loop(4)
+        gpu.main_loop(4)
+        gpu.sync()
+        compare_state(gpu, orc)
