@@ -60,6 +60,7 @@ class Params(ct.Structure):
         ("w", ct.c_double), ("m0", ct.c_double),
         ("radius", ct.c_double), ("xc", ct.c_double), ("yc", ct.c_double),
         ("refin_tol", ct.c_double), ("deref_tol", ct.c_double),
+        ("hydrostatic_start", ct.c_int32),
     ]
 
     def as_dict(self):
@@ -104,11 +105,13 @@ def bubble_params(base_x: int, base_y: int, levels: int, radius: float, xc: floa
                   yc: float, rho_ratio: float, visc_ratio: float, eo: float, mo: float,
                   w: float = 4.0, m0: float = 0.02, refin_tol: float = 1e-3,
                   deref_tol: float = 5e-4, regrid_every: int = 1, n: int = 16,
-                  max_blks: int | None = None) -> Params:
+                  max_blks: int | None = None, gy: float = 0.000005,
+                  hydrostatic_start: int = 1) -> Params:
     """A rising-bubble workload on a base grid of base_x x base_y cells in
     n x n blocks with `levels` refinement levels above the base (finest cell =
     1 length unit, so the base cell size is 2**levels). minLevels = 0: base
-    blocks may stay leaves."""
+    blocks may stay leaves. hydrostatic_start=1: the start-up pressure carries
+    the light phase's hydrostatic head (amrlbm_params.hydrostatic_start)."""
     assert base_x % n == 0 and base_y % n == 0
     nbx, nby = base_x // n, base_y // n
     if max_blks is None:
@@ -116,27 +119,40 @@ def bubble_params(base_x: int, base_y: int, levels: int, radius: float, xc: floa
     return Params(nx=n, ny=n, nbx=nbx, nby=nby, dx0=2 ** levels, min_levels=0,
                   max_levels=levels, max_blks=max_blks, regrid_every=regrid_every,
                   rho_l=1.0 / rho_ratio, rho_h=1.0, visc_ratio=visc_ratio, bo=eo,
-                  ar=archimedes(eo, mo), gy=0.000005, w=w, m0=m0, radius=radius,
-                  xc=xc, yc=yc, refin_tol=refin_tol, deref_tol=deref_tol)
+                  ar=archimedes(eo, mo), gy=gy, w=w, m0=m0, radius=radius,
+                  xc=xc, yc=yc, refin_tol=refin_tol, deref_tol=deref_tol,
+                  hydrostatic_start=hydrostatic_start)
 
 
 def workload_small() -> Params:
     """Plain FP64 rising bubble: base grid 64x128 cells in 16x16 blocks, 2
     refinement levels (finest-equivalent 256x512), R=32 at (128,128),
     density ratio 10, viscosity ratio 10, Eo=10, Mo=1e-3, W=4, M=0.02,
-    refine where |grad C| > 1e-3 (derefine tolerance 5e-4, half the refine
-    tolerance as in the reference's 0.002/0.001)."""
+    Gy=5e-6 (the reference's), hydrostatic start-up pressure, refine where
+    |grad C| > 1e-3 (derefine tolerance 5e-4, half the refine tolerance as in
+    the reference's 0.002/0.001), regrid every step."""
     return bubble_params(64, 128, 2, 32.0, 128.0, 128.0, 10.0, 10.0, 10.0, 1e-3,
                          w=4.0, m0=0.02, refin_tol=1e-3, deref_tol=5e-4, regrid_every=1)
+
+
+# Gravity of the large workload: with Gy = 2.5e-7, D = 256 and Ar = 100 the
+# product Gy*D**3/Ar**2, and with it both phases' viscosities and relaxation
+# times (tau_h = 0.0614, tau_l = 0.614), equal the reference's own start-up
+# bubble's (Gy = 5e-6, D = 51.2, Ar = 40; AMR_Rising_2D_OMP.f90:241-255).
+# At the reference's Gy = 5e-6 the light phase's tau_l = 2.75 and it blows up
+# on the dx=2 level within 2000 steps.
+LARGE_GY = 2.5e-7
 
 
 def workload_large() -> Params:
     """Plain FP64 rising bubble at scale: base grid 256x512 cells in 16x16
     blocks, 3 refinement levels (finest-equivalent 2048x4096), R=128 at
     (1024,512), density ratio 1000, viscosity ratio 100, Eo=10, Mo=1e-5, W=4,
-    regrid every 10 steps (mobility and tolerances as the small workload)."""
+    Gy=2.5e-7 (LARGE_GY), hydrostatic start-up pressure, regrid every 10
+    steps (mobility and tolerances as the small workload)."""
     return bubble_params(256, 512, 3, 128.0, 1024.0, 512.0, 1000.0, 100.0, 10.0, 1e-5,
-                         w=4.0, m0=0.02, refin_tol=1e-3, deref_tol=5e-4, regrid_every=10)
+                         w=4.0, m0=0.02, refin_tol=1e-3, deref_tol=5e-4, regrid_every=10,
+                         gy=LARGE_GY)
 
 
 class AmrLbmError(RuntimeError):
@@ -168,6 +184,7 @@ def load_library(path: str | None = None):
         "amrlbm_destroy": (ct.c_int, [vp]),
         "amrlbm_set_physics": (ct.c_int, [vp, ct.POINTER(Physics)]),
         "amrlbm_set_g_collision": (ct.c_int, [vp, ct.c_int32]),
+        "amrlbm_set_wait_test": (ct.c_int, [vp, ct.c_int32, ct.c_int32]),
         "amrlbm_last_error": (ct.c_char_p, [vp]),
         "amrlbm_device_bytes": (ct.c_int64, [vp]),
         "amrlbm_get_counts": (ct.c_int, [vp, i32p]),
@@ -295,6 +312,11 @@ class AmrLbm:
 
     def set_physics(self, phys: Physics):
         self._check(self.lib.amrlbm_set_physics(self.ctx, ct.byref(phys)))
+
+    def set_wait_test(self, spin_limit: int = 0, hold_block: int = 0):
+        """Failure-detection hook of the level-ordered fills' bounded flag
+        waits (amrlbm_set_wait_test); (0, 0) restores normal operation."""
+        self._check(self.lib.amrlbm_set_wait_test(self.ctx, int(spin_limit), int(hold_block)))
 
     def set_g_collision(self, model: int):
         """G_MRT (MRT_Collision_AMR, the reference's) or G_BGK

@@ -387,7 +387,7 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     if (p->nx < 4 || p->ny < 4 || (p->nx % 2) || (p->ny % 2) || p->nx * p->ny > 1024 ||
         p->nbx < 1 || p->nby < 1 || p->dx0 < 1 || p->min_levels < 0 ||
         p->max_levels < p->min_levels || p->max_levels >= AMR_MAXLV - 1 || p->max_blks < 1 ||
-        p->max_blks < p->nbx * p->nby)
+        p->max_blks < p->nbx * p->nby || p->hydrostatic_start < 0 || p->hydrostatic_start > 1)
         return AMRLBM_ERR_ARG;
     if ((p->dx0 >> p->max_levels) < 1) return AMRLBM_ERR_ARG;  // dx stays an integer >= 1
     if (p->dx0 & (p->dx0 - 1)) return AMRLBM_ERR_ARG;  // powers of two (L0/nx = 2**maxLevels)
@@ -414,6 +414,8 @@ int amrlbm_create(const amrlbm_params* p, amrlbm_ctx** out) {
     s.ny = ny;
     s.max_blks = p->max_blks;
     s.fl_cap = p->max_blks / 4 + 2;
+    s.spin_limit = AMR_SPIN_LIMIT;
+    s.hold_flag = 0;
     s.ap = nx + 2;                   // columns 0..nx+1 (nx even: rows and planes
     s.aplane = (ny + 2) * s.ap;      // of 16-byte multiples)
     s.bplane = nx * ny;
@@ -550,6 +552,15 @@ int amrlbm_set_physics(amrlbm_ctx* ctx, const amrlbm_physics* phys) {
 int amrlbm_set_g_collision(amrlbm_ctx* ctx, int32_t model) {
     if (!ctx || (model != AMRLBM_G_MRT && model != AMRLBM_G_BGK)) return AMRLBM_ERR_ARG;
     ctx->s.g_model = model;
+    drop_graphs(ctx);
+    return AMRLBM_OK;
+}
+
+int amrlbm_set_wait_test(amrlbm_ctx* ctx, int32_t spin_limit, int32_t hold_block) {
+    if (!ctx || spin_limit < 0 || hold_block < 0 || hold_block > ctx->prm.max_blks)
+        return AMRLBM_ERR_ARG;
+    ctx->s.spin_limit = spin_limit > 0 ? spin_limit : AMR_SPIN_LIMIT;
+    ctx->s.hold_flag = hold_block;
     drop_graphs(ctx);
     return AMRLBM_OK;
 }
@@ -810,7 +821,7 @@ int amrlbm_init_fields(amrlbm_ctx* ctx) {
                                   C.data(), nullptr, nullptr, nullptr))
             return r;
     }
-    launch_init_fields(ctx->s, ctx->lc, ctx->st, R);
+    launch_init_fields(ctx->s, ctx->lc, ctx->st, R, ctx->prm.hydrostatic_start, Y0);
     ctx->tail_done = true;
     return sync_check(ctx);
 }
@@ -1260,10 +1271,17 @@ extern "C" int amrlbm_download_fields_noalloc(amrlbm_ctx* ctx, int32_t n, const 
     if (e != cudaSuccess) rc = AMRLBM_ERR_CUDA;
     if (rc == AMRLBM_OK) {  // a pending device-side error status, as the other calls report it
         int st[2] = {0, 0};
-        if (cudaMemcpy(st, &ctx->s.cnt->error, sizeof(st), cudaMemcpyDeviceToHost) != cudaSuccess)
+        if (cudaMemcpy(st, &ctx->s.cnt->error, sizeof(st), cudaMemcpyDeviceToHost) != cudaSuccess) {
             rc = AMRLBM_ERR_CUDA;
-        else if (st[0] != 0)
+        } else if (st[0] != 0) {
+            // reported once, then cleared as amrlbm_download_fields does, by a
+            // copy from this stack array (no allocation)
             rc = st[0];
+            const int zero[2] = {0, 0};
+            if (cudaMemcpy(&ctx->s.cnt->error, zero, sizeof(zero), cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+                rc = AMRLBM_ERR_CUDA;
+        }
     }
     if (prev != pa.device) cudaSetDevice(prev);
     return rc;

@@ -60,6 +60,10 @@ enum { NBI_STRIDE = 64, PLAN_INTS = 10 };
 //   C      : order parameter with both ghost rings, [blk][y+1][col],
 //            col = x+3 (x = -1..nx+2), y = -1..ny+2
 //   P,Ux,Uy: [blk][y][x], x,y = 1..nx,ny
+// default bound of a flag wait of the level-ordered fills: iterations of
+// about 64 ns, about a second in all
+constexpr int AMR_SPIN_LIMIT = 20000000;
+
 struct DevState {
     int nx, ny, max_blks, fl_cap;
     int ap, aplane;  // A row pitch and plane stride (doubles)
@@ -88,6 +92,8 @@ struct DevState {
     int *ref_list, *ref_c1, *der_list;
     Counters* cnt;
     unsigned* queue;  // [4*NQUEUES]: per queue fill claims, consumer claims, CTAs done
+    int spin_limit;   // iterations of a flag wait of the level-ordered fills
+    int hold_flag;    // test hook: this block's ring flag is never raised (0: none)
     PhysD ph;
 };
 

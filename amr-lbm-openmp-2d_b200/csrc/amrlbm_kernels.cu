@@ -36,7 +36,9 @@ __device__ __forceinline__ void ring1_xy(int r, int nx, int ny, int& x, int& y) 
 }
 
 // Initialize_AMR_Rising_Bubble (AMR_Rising_2D_OMP.f90:186-226) given C
-__global__ void __launch_bounds__(256) k_init_fields(DevState s, double R) {
+// hydro != 0: P also carries the light phase's hydrostatic head about the
+// bubble centre y0, Gy*(Rhoh-Rhol)*(1-C)*(y-y0) (amrlbm_params.hydrostatic_start)
+__global__ void __launch_bounds__(256) k_init_fields(DevState s, double R, int hydro, double Y0) {
     extern __shared__ double T[];
     const int nleaf = s.cnt->nleaf, nx = s.nx, ny = s.ny, TW = nx + 4;
     const PhysD& ph = s.ph;
@@ -50,7 +52,11 @@ __global__ void __launch_bounds__(256) k_init_fields(DevState s, double R) {
             auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 1) * TW + (x + ddx + 1)]; };
             const double Cij = Cs(0, 0);
             const double Ux = 0, Uy = 0;
-            const double P = -ph.Sigma / R * Cij;
+            double P = -ph.Sigma / R * Cij;
+            if (hydro) {
+                const double Yc = (double)(s.bj[n] * dx * ny) + dx * (y - 0.5);
+                P = P + ph.Gy * (ph.Rhoh - ph.Rhol) * (1.0 - Cij) * (Yc - Y0);
+            }
             s.Ux[p_idx(s, n, x, y)] = Ux;
             s.Uy[p_idx(s, n, x, y)] = Uy;
             s.P[p_idx(s, n, x, y)] = P;
@@ -679,7 +685,7 @@ __global__ void k_diag_blocks(DevState s, double* part) {
                     const double uy = sh[nc + (j - 1) * nx + (i - 1)];
                     umax = fmax(umax, fabs(uy));
                     const double yc = (double)(s.bj[n] * dx * ny) + dx * (j - 0.5);
-                    const double wgt = (1.0 - C) * a;
+                    const double wgt = (C < 0.5) ? (1.0 - C) * a : 0.0;
                     vol = vol + wgt;
                     ysum = ysum + wgt * yc;
                     vsum = vsum + wgt * uy;
@@ -765,8 +771,9 @@ void launch_minmax(const DevState& s, cudaStream_t st) {
     count_launches(1);
 }
 
-void launch_init_fields(const DevState& s, const LaunchCfg& lc, cudaStream_t st, double radius) {
-    k_init_fields<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s, radius);
+void launch_init_fields(const DevState& s, const LaunchCfg& lc, cudaStream_t st, double radius,
+                        int hydro, double y0) {
+    k_init_fields<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s, radius, hydro, y0);
     count_launches(1);
 }
 

@@ -32,7 +32,8 @@ void launch_macro_h(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_macro_g(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_err(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_minmax(const DevState& s, cudaStream_t st);
-void launch_init_fields(const DevState& s, const LaunchCfg& lc, cudaStream_t st, double radius);
+void launch_init_fields(const DevState& s, const LaunchCfg& lc, cudaStream_t st, double radius,
+                        int hydro, double y0);
 void launch_regrid_flags(const DevState& s, cudaStream_t st, double refin_tol, double deref_tol);
 void launch_restrict(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 // mode 0: Refine_Derefine_Mesh; 1: Initial_Mesh level (no data movement);

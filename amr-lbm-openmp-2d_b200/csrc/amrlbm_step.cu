@@ -28,8 +28,6 @@ void count_launches(int n);
 
 namespace {
 
-constexpr int kSpinLimit = 20000000;  // x ~64 ns: about a second
-
 __device__ __forceinline__ int ld_acquire_i(const int* p) {
     int v;
     asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -483,8 +481,8 @@ __device__ void queue_done(const DevState& s, int q) {
 }
 
 // bounded spin of one thread until *flag is set; false if it ran out
-__device__ __forceinline__ bool spin_flag(const int* flag) {
-    for (int it = 0; it < kSpinLimit; ++it) {
+__device__ __forceinline__ bool spin_flag(const int* flag, int limit) {
+    for (int it = 0; it < limit; ++it) {
         if (ld_acquire_i(flag) != 0) return true;
         __nanosleep(32);
     }
@@ -496,7 +494,7 @@ __device__ __forceinline__ bool spin_flag(const int* flag) {
 __device__ __forceinline__ void wait_coarse(const DevState& s, int q, const NbInfo& nbi) {
     const int t = threadIdx.x;
     if (t < 8 && ((nbi.wait[q] >> (t + 1)) & 1))
-        if (!spin_flag(fill_flags(s, q) + nbi.id[t + 1])) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, q);
+        if (!spin_flag(fill_flags(s, q) + nbi.id[t + 1], s.spin_limit)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, q);
     __syncthreads();
 }
 
@@ -504,7 +502,7 @@ __device__ __forceinline__ void wait_coarse(const DevState& s, int q, const NbIn
 // writes. The release store is cumulative: it orders every write of the CTA
 // that the barrier ordered before thread 0's store.
 __device__ __forceinline__ void publish_ring(const DevState& s, int q, int n) {
-    if (threadIdx.x == 0) st_release_i(fill_flags(s, q) + n, 1);
+    if (threadIdx.x == 0 && n != s.hold_flag) st_release_i(fill_flags(s, q) + n, 1);
 }
 
 // generic-proxy writes seen through an acquire, before bulk copies read them
@@ -1299,7 +1297,7 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
     auto start_tile = [&](int st, int c, int nn, bool block) {
         if (fast) {
         } else if (block) {
-            if (!spin_flag(flags + nn)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
+            if (!spin_flag(flags + nn, s.spin_limit)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
         } else if (ld_acquire_i(flags + nn) == 0) {
             return false;
         }
@@ -1502,7 +1500,7 @@ __global__ void __launch_bounds__(256, 3) k_fill_hg_stream(DevState s, int wr) {
         const int n = __ldg(s.lvl_leaf + c);
         if (t == 0) {
             const unsigned cn = atomicAdd(&s.queue[4 * q + 1], 1u);
-            if (!spin_flag(flags + n)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
+            if (!spin_flag(flags + n, s.spin_limit)) set_error(s, 8 /*AMRLBM_ERR_TIMEOUT*/, 200 + q);
             copy_planes(n);
             s_next = (int)cn;
         }

@@ -21,6 +21,14 @@ e2e      = the same updates timed around upload of every leaf's fields from
            the diagnostics, all through the C ABI (wall clock)
 --impl reference: the oracle (a C++/OpenMP restatement of the reference's
            Fortran, which cannot be compiled here) on all host cores.
+
+Every leg checks that the state it ends on is physical (finite leaf values,
+|Uy| far below the lattice sound speed, positive density, a rising bubble)
+and stops with an error otherwise. cpu_baseline: the oracle is loaded with the
+device's state at the start of the timed region, runs the same regrid
+intervals on all host cores (its diagnostics must then equal the device's bit
+for bit) and goes on to a bounded sample; a second leg runs at 4 threads, the
+reference's OMP_NUM_THREADS (AMR_Rising_2D_OMP.f90:23).
 """
 from __future__ import annotations
 
@@ -72,9 +80,29 @@ def config_dict(p, inner):
     return {"workload": WORKLOAD, "base_grid": "256x512", "block": f"{p.nx}x{p.ny}",
             "levels": p.max_levels, "finest_equivalent": "2048x4096", "radius": p.radius,
             "density_ratio": round(p.rho_h / p.rho_l, 6), "viscosity_ratio": p.visc_ratio,
-            "eo": p.bo, "mo": 1e-5, "w": p.w, "regrid_every": p.regrid_every,
+            "eo": p.bo, "mo": 1e-5, "w": p.w, "m0": p.m0, "gy": p.gy,
+            "start_pressure": "hydrostatic" if p.hydrostatic_start else "laplace",
+            "regrid_every": p.regrid_every,
             "time_steps_per_bench_step": inner, "l2": "flushed between bench steps",
             "parallelism": "replicas"}
+
+
+# bound on max |Uy| of a physical state of the workload: 5000 steps of it stay
+# below 0.002 (tests/test_physics_long.py), the lattice sound speed is 0.577
+U_BOUND = 0.05
+
+
+def check_state(d, label):
+    """Stops the bench unless the diagnostics (amrlbm_diag / the oracle's
+    Output) describe a physical state."""
+    import math
+    bad = [k for k in ("mass", "rho_min", "u_max", "y_centroid", "rise_velocity")
+           if not math.isfinite(d[k])]
+    if d.get("status", 0) or bad:
+        raise RuntimeError(f"{label}: non-finite state {bad} {d}")
+    if not (d["u_max"] < U_BOUND and d["rho_min"] > 0.0 and d["rise_velocity"] > 0.0):
+        raise RuntimeError(f"{label}: state not physical: u_max {d['u_max']}, rho_min "
+                           f"{d['rho_min']}, rise velocity {d['rise_velocity']}")
 
 
 def measured_peak():
@@ -196,23 +224,45 @@ def allreduce(vals, op, world, device=None):
     return t.tolist()
 
 
-def cpu_baseline_run(p, inner, seconds, max_chunks=400):
-    """The oracle on every host core: chunks of `inner` time steps until
-    `seconds` of CPU work (bounded sample of the same workload)."""
+def oracle_from_device(gpu, p, threads):
+    """An oracle holding the device pool's complete state (topology, free
+    list, level range, every allocated block's fields)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import numpy as np
+    from amrlbm import F_ALLOC
     from oracle_lib import Oracle
-    threads = os.cpu_count() or 1
     orc = Oracle(p, threads)
-    orc.initialize_rising_bubble()
+    t = gpu.topology()
+    c = gpu.counts()
+    orc.set_topology(t, c["kk"])
+    orc.set_level_range(c["level_min"], c["level_max"])
+    ids = np.array([i + 1 for i in range(len(t["level"])) if t["flags"][i] & F_ALLOC],
+                   dtype=np.int32)
+    f = gpu.download_fields(ids)
+    shp = dict(h=gpu.hshape, g=gpu.hshape, C=gpu.cshape, P=gpu.pshape, Ux=gpu.pshape,
+               Uy=gpu.pshape)
+    for i, bid in enumerate(ids):
+        orc.upload_block(int(bid), *[f[k][i].reshape(shp[k], order="F")
+                                     for k in ("h", "g", "C", "P", "Ux", "Uy")])
+    return orc
+
+
+def cpu_leg(orc, p, inner, seconds, min_chunks=0, check_after=None):
+    """Regrid intervals of the oracle until `seconds` of CPU work (at least
+    min_chunks); after chunk `check_after[0]` its diagnostics are handed to
+    check_after[1]. Returns MLUPS, chunks, seconds."""
     updates, elapsed, chunks = 0, 0.0, 0
-    while elapsed < seconds and chunks < max_chunks:
+    while chunks < min_chunks or elapsed < seconds:
         nleaf = orc.counts()["nleaf"]
         t = time.perf_counter()
         orc.main_loop(inner)
         elapsed += time.perf_counter() - t
         updates += nleaf * p.nx * p.ny * inner  # the regrid is after the last step
         chunks += 1
-    return updates / elapsed / 1e6, threads, chunks, elapsed
+        if check_after and chunks == check_after[0]:
+            check_after[1](orc.output())
+    check_state(orc.output(), f"oracle after {chunks} intervals")
+    return updates / elapsed / 1e6, chunks, elapsed
 
 
 def run_reference(args):
@@ -228,6 +278,7 @@ def run_reference(args):
     orc.initialize_rising_bubble()
     for _ in range(args.warmup):
         orc.main_loop(inner)
+    check_state(orc.output(), "reference arm after warm-up")
     updates, total = 0, 0.0
     for _ in range(args.steps):
         nleaf = orc.counts()["nleaf"]
@@ -235,6 +286,7 @@ def run_reference(args):
         orc.main_loop(inner)
         total += time.perf_counter() - t
         updates += nleaf * p.nx * p.ny * inner
+    check_state(orc.output(), "reference arm after the timed steps")
     v = updates / total / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -269,6 +321,11 @@ def run_own(args):
     for _ in range(args.warmup):
         gpu.main_loop(inner)
     gpu.sync()
+    check_state(gpu.output(), "after warm-up")
+    # the oracle takes the state the timed region starts from (rank 0, N=1)
+    orc = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        orc = oracle_from_device(gpu, p, os.cpu_count() or 1)
 
     def barrier():
         gpu.sync()
@@ -295,6 +352,8 @@ def run_own(args):
     barrier()
     launches = gpu.launch_count() - launches0
     updates = gpu.profile_read(0)[2] - cells0
+    diag_timed = gpu.output()
+    check_state(diag_timed, "after the timed region")
 
     # ---- the same steps once more with CUDA events around each kernel group,
     # for the per-kernel split and the roofline of the dominant kernel
@@ -309,6 +368,7 @@ def run_own(args):
         ms, n, _ = gpu.profile_read(k)
         kern[k] = (name, bpc, ms, n)
     gpu.profile(False)
+    check_state(gpu.output(), "after the per-kernel pass")
     max_ms = allreduce([total_ms], _op("max"), world, dev)[0]
     all_updates = allreduce([float(updates)], _op("sum"), world, dev)[0]
     value = all_updates / (max_ms / 1e3) / 1e6
@@ -348,6 +408,7 @@ def run_own(args):
             diag = gpu.output()
             d2h += sum(a.nbytes for a in state.values()) + ids.nbytes + 8 * len(diag)
             t_e2e += time.perf_counter() - t
+            check_state(diag, "end-to-end step")
         barrier()
         _, _, u1 = gpu.profile_read(0)
         t_max = allreduce([t_e2e], _op("max"), world, dev)[0]
@@ -381,18 +442,34 @@ def run_own(args):
                       "avg_us": round(v[2] / max(v[3], 1) * 1e3, 2),
                       "share": round(v[2] / total_prof, 4)} for v in kern.values()}
 
-    cpu = None
-    if not args.no_cpu_baseline and world >= 1:
-        v, threads, chunks, el = cpu_baseline_run(workload(), inner, args.cpu_seconds)
+    cpu = cpu4 = None
+    if orc is not None:
+        def same_as_device(d):
+            for k, v in diag_timed.items():
+                if d[k] != v:
+                    raise RuntimeError(f"oracle differs from the device over the timed "
+                                       f"window: {k} {d[k]} != {v}")
+        threads = os.cpu_count() or 1
+        v, chunks, el = cpu_leg(orc, p, inner, args.cpu_seconds, min_chunks=args.steps,
+                                check_after=(args.steps, same_as_device))
         cpu = {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port",
-               "sample": f"{chunks} x {inner} time steps of the same workload from its "
-                         f"start-up state ({el:.1f} s)"}
+               "sample": f"{chunks} x {inner} time steps from the state the timed region "
+                         f"started from ({el:.1f} s); after the first {args.steps} "
+                         f"intervals its diagnostics equalled the device's bit for bit",
+               "parity_over_timed_window": "bit-exact"}
+        orc.set_threads(4)
+        v4, chunks4, el4 = cpu_leg(orc, p, inner, args.cpu_seconds / 2)
+        cpu4 = {"value": v4, "unit": "MLUPS", "cores": 4, "kind": "port",
+                "sample": f"the next {chunks4} x {inner} time steps ({el4:.1f} s) at 4 threads, "
+                          f"the reference's OMP_NUM_THREADS"}
+        orc.close()
     line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (analytic rising bubble of the reference start-up)",
             "config": config_dict(p, inner), "hbm_gbs": value * 1e6 * BYTES_PER_UPDATE / 1e9,
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "roofline": roofline, "cpu_baseline": cpu, "cpu_baseline_4_threads": cpu4,
+            "e2e": e2e, "clocks": clk,
             "gpu_launches": int(launches), "kernels": kernels,
             "leaf_cells_per_step": updates / (args.steps * inner),
             "diagnostics": {k: diag[k] for k in ("mass", "y_centroid", "rise_velocity")}}

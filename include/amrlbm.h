@@ -87,6 +87,15 @@ typedef struct amrlbm_params {
     double radius, xc, yc;   /* bubble radius and centre (finest-cell units)          */
     double refin_tol;        /* refine if Err_Interface > refin_tol                   */
     double deref_tol;        /* derefine if all 4 children's error <= deref_tol       */
+    /* Start-up pressure of Initialize_AMR_Rising_Bubble. 0 (the reference's,
+     * AMR_Rising_2D_OMP.f90:193): the Laplace jump P = -Sigma/R*C.
+     * 1: the same plus the hydrostatic head of the light phase about the
+     * bubble centre, Gy*(Rhoh-Rhol)*(1-C)*(y-yc). The buoyancy force
+     * Fb = (Rhoh-Rho)*Gy (LBM_Subroutines.f90:152) already removes the heavy
+     * phase's head, so P stays uniform there, and inside the bubble the
+     * head balances Fb from the first step instead of accelerating the light
+     * phase from rest. */
+    int32_t hydrostatic_start;
 } amrlbm_params;
 
 /* Derived physical constants (D2Q9_Mod.f90:13-16), as computed by
@@ -112,6 +121,16 @@ int amrlbm_set_physics(amrlbm_ctx* ctx, const amrlbm_physics* phys);
  * the reference keeps commented out at :180. */
 enum { AMRLBM_G_MRT = 0, AMRLBM_G_BGK = 1 };
 int amrlbm_set_g_collision(amrlbm_ctx* ctx, int32_t model);
+/* Failure-detection test hook; no counterpart in the reference, whose
+ * OpenMP barriers cannot time out. The level-ordered fills (a level range
+ * narrower than the leaves) order their items by per-block flags, and every
+ * wait on a flag is bounded: when it runs out the kernel records
+ * AMRLBM_ERR_TIMEOUT, goes on and returns, and the next synchronising call
+ * reports it. spin_limit > 0 replaces the bound (iterations of about 64 ns;
+ * 0 restores the default of about a second); hold_block > 0 makes the fills
+ * never raise that block's flag, so that every item waiting for it runs out
+ * of its bound. (0, 0) restores normal operation. */
+int amrlbm_set_wait_test(amrlbm_ctx* ctx, int32_t spin_limit, int32_t hold_block);
 const char* amrlbm_last_error(const amrlbm_ctx* ctx);
 /* Device memory held by the context, bytes. */
 int64_t amrlbm_device_bytes(const amrlbm_ctx* ctx);
@@ -201,11 +220,13 @@ int amrlbm_sync(amrlbm_ctx* ctx);
 
 /* ---- diagnostics -------------------------------------------------------- */
 /* Output (AMR_Rising_2D_OMP.f90:456-489) with a fixed summation order, plus
- * the bubble (C < 1/2) centroid and rise velocity:
+ * the bubble centroid and rise velocity. The bubble sums run over the cells
+ * with C < 1/2 only, so that round-off of C around 1 in the heavy phase, summed
+ * over the whole domain, does not move them:
  *   out[0] mass = sum rho*dx^2       out[1] rho_min   out[2] rho_max
- *   out[3] u_max = max |Uy|          out[4] bubble volume = sum (1-C)*dx^2
- *   out[5] yc = sum (1-C)*y*dx^2 / out[4]
- *   out[6] v_rise = sum (1-C)*Uy*dx^2 / out[4]
+ *   out[3] u_max = max |Uy|          out[4] bubble volume = sum_{C<1/2} (1-C)*dx^2
+ *   out[5] yc = sum_{C<1/2} (1-C)*y*dx^2 / out[4]
+ *   out[6] v_rise = sum_{C<1/2} (1-C)*Uy*dx^2 / out[4]
  *   out[7] phase volume sum C*dx^2
  * Returns AMRLBM_ERR_NAN if any leaf value is not finite. */
 int amrlbm_diag(amrlbm_ctx* ctx, double out[8]);
@@ -252,8 +273,10 @@ int amrlbm_flush_l2(amrlbm_ctx* ctx);
  * nothing runs; split larger downloads into several calls. The scratch is
  * shared by all contexts on a device: calls that overlap in time on one
  * device race on it and must be serialised by the caller. The first call on
- * a device sets the scratch up (no allocation); it returns no message
- * through amrlbm_last_error. */
+ * a device sets the scratch up (no allocation). A pending device error status
+ * (pool full, level jump, ...) is returned once and cleared, as
+ * amrlbm_download_fields does, but without a message through
+ * amrlbm_last_error. */
 #define AMRLBM_NOALLOC_STAGE_DOUBLES 524288 /* 4 MiB */
 #define AMRLBM_NOALLOC_MAX_BLOCKS 16384
 int amrlbm_download_fields_noalloc(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, double* h,

@@ -1484,6 +1484,13 @@ void initialize_rising_bubble(orc_sim& s) {
                 s.Pm(B.Ux, i, j) = 0;
                 s.Pm(B.Uy, i, j) = 0;
                 s.Pm(B.P, i, j) = -ph.Sigma / R * s.Cm(B, i, j);
+                /* optional: the light phase's hydrostatic head about the
+                   bubble centre (amrlbm_params.hydrostatic_start) */
+                if (s.prm.hydrostatic_start) {
+                    const double Yc = (double)(B.J * dx * ny) + dx * (j - 0.5);
+                    s.Pm(B.P, i, j) = s.Pm(B.P, i, j) +
+                                      ph.Gy * (ph.Rhoh - ph.Rhol) * (1.0 - s.Cm(B, i, j)) * (Yc - Y0);
+                }
             }
         std::vector<double> mu;
         chemical_potential(s, dx, B, mu);
@@ -1559,6 +1566,9 @@ orc_sim* orc_create(const amrlbm_params* p, int nthreads) {
 }
 
 void orc_destroy(orc_sim* s) { delete s; }
+void orc_set_threads(orc_sim* s, int nthreads) {
+    s->nthreads = nthreads > 0 ? nthreads : omp_get_max_threads();
+}
 int orc_last_error(const orc_sim* s) { return s->err; }
 int orc_level_jump_count(const orc_sim* s) { return s->level_jumps; }
 
@@ -1804,7 +1814,7 @@ int orc_diag(const orc_sim* s, double out[8]) {
                 const double uy = s->Pm(B.Uy, i, j);
                 U_max = std::fmax(U_max, std::fabs(uy));
                 const double yc = (double)(B.J * dx * s->ny) + dx * (j - 0.5);
-                const double wgt = (1.0 - C) * a;
+                const double wgt = (C < 0.5) ? (1.0 - C) * a : 0.0;
                 bv = bv + wgt;
                 by = by + wgt * yc;
                 bu = bu + wgt * uy;

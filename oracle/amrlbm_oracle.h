@@ -26,6 +26,7 @@ typedef struct orc_sim orc_sim;
 
 orc_sim* orc_create(const amrlbm_params* p, int nthreads);
 void orc_destroy(orc_sim* s);
+void orc_set_threads(orc_sim* s, int nthreads);
 int orc_last_error(const orc_sim* s);       /* sticky AMRLBM_ERR_* code      */
 int orc_level_jump_count(const orc_sim* s); /* "Error in SUB_Fill_*" prints  */
 void orc_physics(const orc_sim* s, amrlbm_physics* out);

@@ -29,6 +29,7 @@ def lib():
         sig = {
             "orc_create": (vp, [ct.POINTER(Params), ct.c_int]),
             "orc_destroy": (None, [vp]),
+            "orc_set_threads": (None, [vp, ct.c_int]),
             "orc_last_error": (ct.c_int, [vp]),
             "orc_level_jump_count": (ct.c_int, [vp]),
             "orc_physics": (None, [vp, ct.POINTER(Physics)]),
@@ -97,6 +98,9 @@ class Oracle:
     hshape = property(lambda self: (9, self.nx + 2, self.ny + 2))
     cshape = property(lambda self: (self.nx + 4, self.ny + 4))
     pshape = property(lambda self: (self.nx, self.ny))
+
+    def set_threads(self, n):
+        self.L.orc_set_threads(self.s, n)
 
     def error(self):
         return self.L.orc_last_error(self.s)

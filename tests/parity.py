@@ -104,3 +104,16 @@ def randomize_leaves(orc, seed, c_lo=-0.1, c_hi=1.1):
         h = w[:, None, None] * rng.uniform(0.0, 1.0, size=b["h"].shape)
         g = w[:, None, None] * rng.uniform(-1e-3, 1e-3, size=b["g"].shape)
         orc.upload_block(int(bid), h, g, C, P, Ux, Uy)
+
+
+def assert_physical(d, u_bound, label=""):
+    """The Output diagnostics of a physical rising-bubble state
+    (AMR_Rising_2D_OMP.f90:456-489): every leaf value finite, the velocity far
+    below the lattice sound speed 1/sqrt(3), the light phase's density
+    positive, the bubble rising."""
+    assert d.get("status", 0) == 0, f"{label}: non-finite values"
+    for k in ("mass", "rho_min", "rho_max", "u_max", "y_centroid", "rise_velocity"):
+        assert np.isfinite(d[k]), f"{label}: {k} = {d[k]}"
+    assert d["u_max"] < u_bound, f"{label}: u_max {d['u_max']} >= {u_bound}"
+    assert d["rho_min"] > 0.0, f"{label}: rho_min {d['rho_min']}"
+    assert d["rise_velocity"] > 0.0, f"{label}: rise velocity {d['rise_velocity']}"

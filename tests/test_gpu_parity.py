@@ -196,26 +196,6 @@ def test_large_workload_topology_and_fields():
         compare_fields(gpu, orc)
 
 
-def test_large_workload_long_run_with_mesh_changes():
-    """The same workload for 400 steps (40 regrids: most change nothing and
-    keep the fill plans, a few refine and derefine), bit for bit, with the
-    mesh checked to have changed along the way."""
-    p = amrlbm.workload_large()
-    orc = Oracle(p)
-    orc.initialize_rising_bubble()
-    with AmrLbm(p) as gpu:
-        gpu.initialize_rising_bubble()
-        start = gpu.leaves().copy()
-        for _ in range(4):
-            orc.main_loop(100)
-            gpu.main_loop(100)
-        gpu.sync()
-        assert not np.array_equal(gpu.leaves(), start)
-        compare_counts(gpu, orc)
-        compare_topology(gpu, orc)
-        compare_fields(gpu, orc)
-
-
 @pytest.mark.parametrize("name", ["reference_default", "small_16x16"])
 def test_device_matches_golden_fixtures(name):
     """The device path against the committed fixtures of tests/golden/
