@@ -39,6 +39,7 @@ ERR_TIMEOUT = 8
 ERR_CAPACITY = 9
 ERR_IO = 10
 G_MRT, G_BGK = 0, 1  # collision models of g (amrlbm_set_g_collision)
+FP64, FP16, BF16 = 0, 1, 2  # storage precisions of amrlbm_step (amrlbm_set_precision)
 
 F_LEAF, F_HASLEAF, F_REFIN, F_DEREF, F_ALLOC = 1, 2, 4, 8, 16
 
@@ -65,6 +66,40 @@ class Params(ct.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Instance(ct.Structure):
+    """``amrlbm_instance`` (include/amrlbm.h): one problem of a batch."""
+
+    _fields_ = [
+        ("nbx", ct.c_int32), ("nby", ct.c_int32), ("dx0", ct.c_int32), ("max_levels", ct.c_int32),
+        ("rho_l", ct.c_double), ("rho_h", ct.c_double), ("visc_ratio", ct.c_double),
+        ("bo", ct.c_double), ("ar", ct.c_double), ("gy", ct.c_double), ("w", ct.c_double),
+        ("m0", ct.c_double), ("radius", ct.c_double), ("xc", ct.c_double), ("yc", ct.c_double),
+        ("hydrostatic_start", ct.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+    @staticmethod
+    def from_params(p: "Params") -> "Instance":
+        """The instance that runs the same problem as one-mesh params p."""
+        return Instance(nbx=p.nbx, nby=p.nby, dx0=p.dx0, max_levels=p.max_levels, rho_l=p.rho_l,
+                        rho_h=p.rho_h, visc_ratio=p.visc_ratio, bo=p.bo, ar=p.ar, gy=p.gy, w=p.w,
+                        m0=p.m0, radius=p.radius, xc=p.xc, yc=p.yc,
+                        hydrostatic_start=p.hydrostatic_start)
+
+    def params(self, batch: "Params") -> "Params":
+        """One-mesh params of this instance under the batch's block size,
+        tolerances and regrid interval (the same problem run alone)."""
+        q = Params(**batch.as_dict())
+        for k in ("nbx", "nby", "dx0", "max_levels", "rho_l", "rho_h", "visc_ratio", "bo", "ar",
+                  "gy", "w", "m0", "radius", "xc", "yc", "hydrostatic_start"):
+            setattr(q, k, getattr(self, k))
+        q.min_levels = 0
+        q.max_blks = tree_blocks(q.nbx, q.nby, q.max_levels)
+        return q
 
 
 class Physics(ct.Structure):
@@ -155,6 +190,60 @@ def workload_large() -> Params:
                          gy=LARGE_GY)
 
 
+# Lattice limits of a batch instance: the relaxation times of both phases
+# and the velocity scale sqrt(Gy D) (lattice Mach number sqrt(3) U)
+TAU_RANGE = (0.02, 2.0)
+U_SCALE = 0.01
+
+
+def batch_instances(count: int = 256, seed: int = 20261203, n: int = 16) -> list:
+    """Seeded batch of uneven rising-bubble problems: base grid uniform in
+    {64x128, 128x256, 256x512} cells, 2 or 3 refinement levels (finest cell 1),
+    R uniform in [16, 96] finest cells (centred in x, at a quarter of the
+    height), density ratio log-uniform in [10, 1000], Eo uniform in [1, 50],
+    Mo log-uniform in [1e-6, 1e-2]; viscosity ratio min(density ratio, 100),
+    W 4, M0 0.02, hydrostatic start. Gy is set per instance for a velocity
+    scale sqrt(Gy D) = U_SCALE; an instance whose relaxation times
+    3 mu/rho leave TAU_RANGE at that gravity cannot be run on the lattice and is
+    drawn again from the same stream."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    bases = [(64, 128), (128, 256), (256, 512)]
+    out = []
+    while len(out) < count:
+        bx, by = bases[int(rng.integers(0, 3))]
+        levels = int(rng.integers(2, 4))
+        radius = float(rng.uniform(16.0, 96.0))
+        ratio = float(10.0 ** rng.uniform(1.0, 3.0))
+        eo = float(rng.uniform(1.0, 50.0))
+        mo = float(10.0 ** rng.uniform(-6.0, -2.0))
+        width, height = bx * 2 ** levels, by * 2 ** levels
+        if 2.5 * radius > width or 2.5 * radius > height / 4.0:
+            continue  # the bubble must fit the domain with room to rise
+        D = 2.0 * radius
+        gy = U_SCALE ** 2 / D
+        visc = min(ratio, 100.0)
+        ar = archimedes(eo, mo)
+        rho_l, rho_h = 1.0 / ratio, 1.0
+        muh = (gy * rho_h * (rho_h - rho_l) * D ** 3) ** 0.5 / ar
+        tau_h, tau_l = 3.0 * muh / rho_h, 3.0 * (muh / visc) / rho_l
+        if not (TAU_RANGE[0] <= tau_h <= TAU_RANGE[1] and TAU_RANGE[0] <= tau_l <= TAU_RANGE[1]):
+            continue
+        out.append(Instance(nbx=bx // n, nby=by // n, dx0=2 ** levels, max_levels=levels,
+                            rho_l=rho_l, rho_h=rho_h, visc_ratio=visc, bo=eo, ar=ar, gy=gy,
+                            w=4.0, m0=0.02, radius=radius, xc=width / 2.0, yc=height / 4.0,
+                            hydrostatic_start=1))
+    return out
+
+
+def batch_params(n: int = 16, max_blks: int = 200000, regrid_every: int = 10) -> Params:
+    """Batch-wide params: block size, pool size, tolerances, regrid interval."""
+    return Params(nx=n, ny=n, nbx=1, nby=1, dx0=1, min_levels=0, max_levels=0,
+                  max_blks=max_blks, regrid_every=regrid_every, refin_tol=1e-3, deref_tol=5e-4,
+                  rho_l=0.1, rho_h=1.0, visc_ratio=10.0, bo=10.0, ar=30.0, gy=5e-6, w=4.0,
+                  m0=0.02, radius=16.0, xc=0.0, yc=0.0)
+
+
 class AmrLbmError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"amrlbm status {status}: {message}")
@@ -185,6 +274,12 @@ def load_library(path: str | None = None):
         "amrlbm_set_physics": (ct.c_int, [vp, ct.POINTER(Physics)]),
         "amrlbm_set_g_collision": (ct.c_int, [vp, ct.c_int32]),
         "amrlbm_set_wait_test": (ct.c_int, [vp, ct.c_int32, ct.c_int32]),
+        "amrlbm_set_precision": (ct.c_int, [vp, ct.c_int32]),
+        "amrlbm_get_fill_order": (ct.c_int, [vp, i32p]),
+        "amrlbm_create_batch": (ct.c_int, [ct.POINTER(Params), ct.c_int32, ct.POINTER(Instance),
+                                           ct.POINTER(vp)]),
+        "amrlbm_get_instances": (ct.c_int, [vp, i32p]),
+        "amrlbm_diag_instances": (ct.c_int, [vp, dp]),
         "amrlbm_last_error": (ct.c_char_p, [vp]),
         "amrlbm_device_bytes": (ct.c_int64, [vp]),
         "amrlbm_get_counts": (ct.c_int, [vp, i32p]),
@@ -255,12 +350,21 @@ def _ptr(a, ctype):
 class AmrLbm:
     """One device-resident block pool, driven like the reference's Main_Loop."""
 
-    def __init__(self, params: Params, lib=None):
+    def __init__(self, params: Params, lib=None, instances=None):
+        """One mesh (params), or a batch of independent problems (instances:
+        a list of Instance; params then gives block size, pool size,
+        tolerances and regrid interval, amrlbm_create_batch)."""
         self.lib = lib or load_library()
         self.params = params
         self.nx, self.ny = params.nx, params.ny
+        self.instances = list(instances) if instances is not None else None
         ctx = ct.c_void_p()
-        st = self.lib.amrlbm_create(ct.byref(params), ct.byref(ctx))
+        if self.instances is None:
+            st = self.lib.amrlbm_create(ct.byref(params), ct.byref(ctx))
+        else:
+            arr = (Instance * len(self.instances))(*self.instances)
+            st = self.lib.amrlbm_create_batch(ct.byref(params), len(self.instances), arr,
+                                              ct.byref(ctx))
         if st != 0:
             raise AmrLbmError(st, "amrlbm_create failed (is a B200 visible?)")
         self.ctx = ctx
@@ -312,6 +416,21 @@ class AmrLbm:
 
     def set_physics(self, phys: Physics):
         self._check(self.lib.amrlbm_set_physics(self.ctx, ct.byref(phys)))
+
+    def set_precision(self, precision):
+        """FP64 (bit for bit with the reference), FP16 or BF16 storage of the
+        populations for main_loop (amrlbm_set_precision); also "fp64",
+        "fp16", "bf16"."""
+        if isinstance(precision, str):
+            precision = {"fp64": FP64, "fp16": FP16, "bf16": BF16}[precision.lower()]
+        self._check(self.lib.amrlbm_set_precision(self.ctx, int(precision)))
+
+    def fill_order(self):
+        """Which ghost fills of the current mesh need level order
+        (amrlbm_get_fill_order): dict c2, c1, hg -> bool."""
+        a = np.zeros(3, dtype=np.int32)
+        self._check(self.lib.amrlbm_get_fill_order(self.ctx, _ptr(a, ct.c_int32)))
+        return dict(zip(("c2", "c1", "hg"), (bool(v) for v in a)))
 
     def set_wait_test(self, spin_limit: int = 0, hold_block: int = 0):
         """Failure-detection hook of the level-ordered fills' bounded flag
@@ -372,6 +491,23 @@ class AmrLbm:
         self._check(self.lib.amrlbm_diag(self.ctx, _ptr(out, ct.c_double)))
         return dict(zip(("mass", "rho_min", "rho_max", "u_max", "bubble_volume",
                          "y_centroid", "rise_velocity", "phase_volume"), out.tolist()))
+
+    def output_instances(self):
+        """Output per instance of a batch (amrlbm_diag_instances): a list of
+        dicts as output()."""
+        ni = len(self.instances) if self.instances else 1
+        out = np.zeros(8 * ni)
+        self._check(self.lib.amrlbm_diag_instances(self.ctx, _ptr(out, ct.c_double)))
+        keys = ("mass", "rho_min", "rho_max", "u_max", "bubble_volume", "y_centroid",
+                "rise_velocity", "phase_volume")
+        return [dict(zip(keys, out[8 * i:8 * i + 8].tolist())) for i in range(ni)]
+
+    def block_instances(self):
+        """Instance (0-based) of blocks 1..Nblks."""
+        n = self.counts()["nblks"]
+        a = np.zeros(max(n, 1), dtype=np.int32)
+        self._check(self.lib.amrlbm_get_instances(self.ctx, _ptr(a, ct.c_int32)))
+        return a[:n]
 
     # -- state -------------------------------------------------------------
     def counts(self):

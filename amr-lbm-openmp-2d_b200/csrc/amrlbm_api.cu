@@ -3,6 +3,7 @@
 // driver's start-up, CUDA-graph stepping, diagnostics and timing.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -53,6 +54,11 @@ struct amrlbm_ctx {
     long long launches0 = 0;
     long long captured = 0, replayed = 0;  // graph kernels: captured once, run per replay
     GraphEntry* prof_pending = nullptr;    // replayed with profiling, events not read yet
+    // mixed precision (amrlbm_set_precision): which state is current
+    bool mp_stale = true;     // the FP64 pool is newer than the mixed-precision state
+    bool fp64_stale = false;  // the mixed-precision state is newer than the FP64 pool
+    std::vector<amrlbm_instance> insts;  // batched instances (amrlbm_create_batch)
+    unsigned char* d_active = nullptr;   // s.inst_active
 };
 
 namespace {
@@ -108,6 +114,28 @@ PhysD to_physd(const amrlbm_physics& p) {
     d.tauh5 = d.tauh + 0.5;
     d.yW = 1.0 / d.W;
     return d;
+}
+
+PhysF to_physf(const PhysD& d) {
+    PhysF f;
+    f.W = (float)d.W;
+    f.iW = (float)(1.0 / d.W);
+    f.Beta4 = (float)d.Beta4;
+    f.kappa = (float)d.kappa;
+    f.M0 = (float)d.M0;
+    f.wc = (float)d.wc;
+    f.omwc = (float)d.omwc;
+    f.Rhol = (float)d.Rhol;
+    f.Rhoh = (float)d.Rhoh;
+    f.dRho = (float)d.dRho;
+    f.dRho3 = (float)d.dRho3;
+    f.dRho6 = (float)d.dRho6;
+    f.Gy = (float)d.Gy;
+    f.itau_d = (float)d.itau_d;
+    f.itaul = (float)d.itaul;
+    f.taul5 = (float)d.taul5;
+    f.tauh5 = (float)d.tauh5;
+    return f;
 }
 
 // ---- field transfer kernels (reference layouts <-> pool layouts) ----------
@@ -275,9 +303,51 @@ struct ProfMark {
     }
 };
 
+// Refine_Derefine_Mesh in a mixed-precision run: the flags from the err that
+// the tail computed, and the FP64 restriction (Restrict.f90, FP64 sums) and
+// prolongation kernels on FP64 copies of just the blocks they read, converted
+// to FP64 before and back after.
+void enqueue_regrid_mp(amrlbm_ctx* ctx, double rt, double dt) {
+    const DevState& s = ctx->s;
+    launch_regrid_flags(s, ctx->st, rt, dt);
+    launch_mp_convert(s, ctx->lc, ctx->st, 2, 0);  // children of derefined parents
+    launch_restrict(s, ctx->lc, ctx->st);
+    launch_mp_convert(s, ctx->lc, ctx->st, 1, 1);  // the derefined parents
+    launch_regrid_topo(s, ctx->st, 0, -1, -1, 1);
+    launch_build_plans(s, ctx->lc, ctx->st);
+    launch_mp_convert(s, ctx->lc, ctx->st, 3, 0);  // refined parents
+    launch_prolong(s, ctx->lc, ctx->st);
+    launch_mp_convert(s, ctx->lc, ctx->st, 4, 1);  // their new children
+}
+
+void enqueue_step_mp(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail, bool regrid,
+                     bool last) {
+    const DevState& s = ctx->s;
+    {
+        ProfMark m(ctx, ge, 0);
+        launch_mp_collide(s, ctx->lc, ctx->st, prev_tail, last ? 1 : 0);
+    }
+    {
+        ProfMark m(ctx, ge, 1);
+        launch_mp_fill_hg_stream(s, ctx->lc, ctx->st, last ? 1 : 0);
+    }
+    if (tail) {
+        ProfMark m(ctx, ge, 2);
+        launch_mp_tail(s, ctx->lc, ctx->st);
+    }
+    if (regrid) {
+        ProfMark m(ctx, ge, 3);
+        enqueue_regrid_mp(ctx, ctx->prm.refin_tol, ctx->prm.deref_tol);
+    }
+}
+
 void enqueue_step(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail, bool regrid,
                   bool last) {
     const DevState& s = ctx->s;
+    if (s.mp.fmt) {
+        enqueue_step_mp(ctx, ge, prev_tail, tail, regrid, last);
+        return;
+    }
     {
         ProfMark m(ctx, ge, 0);
         launch_fill_c(s, ctx->lc, ctx->st, 2, prev_tail ? CONS_COLLIDE_READ : CONS_COLLIDE_FUSED,
@@ -542,9 +612,22 @@ void drop_graphs(amrlbm_ctx* ctx) {
     ctx->prof_pending = nullptr;
 }
 
+// The FP64 pool made current (converted back from the mixed-precision state
+// after amrlbm_step ran in FP16/BF16) before a call that reads or writes it;
+// `writes`: the call changes the FP64 state, which the next mixed-precision
+// step then converts again.
+void ensure_fp64(amrlbm_ctx* ctx, bool writes) {
+    if (ctx->s.mp.fmt && ctx->fp64_stale) {
+        launch_mp_convert(ctx->s, ctx->lc, ctx->st, 0, 0);
+        ctx->fp64_stale = false;
+    }
+    if (writes) ctx->mp_stale = true;
+}
+
 int amrlbm_set_physics(amrlbm_ctx* ctx, const amrlbm_physics* phys) {
     if (!ctx || !phys) return AMRLBM_ERR_ARG;
     ctx->s.ph = to_physd(*phys);
+    ctx->s.mp.ph = to_physf(ctx->s.ph);
     drop_graphs(ctx);
     return AMRLBM_OK;
 }
@@ -553,6 +636,59 @@ int amrlbm_set_g_collision(amrlbm_ctx* ctx, int32_t model) {
     if (!ctx || (model != AMRLBM_G_MRT && model != AMRLBM_G_BGK)) return AMRLBM_ERR_ARG;
     ctx->s.g_model = model;
     drop_graphs(ctx);
+    return AMRLBM_OK;
+}
+
+int amrlbm_set_precision(amrlbm_ctx* ctx, int32_t precision) {
+    if (!ctx || precision < AMRLBM_FP64 || precision > AMRLBM_BF16) return AMRLBM_ERR_ARG;
+    DevState& s = ctx->s;
+    if (precision != AMRLBM_FP64 && (s.nx != s.ny || (s.nx != 8 && s.nx != 16)))
+        return fail(ctx, AMRLBM_ERR_ARG, "mixed precision needs 8x8 or 16x16 blocks");
+    if (precision == s.mp.fmt) return AMRLBM_OK;
+    ensure_fp64(ctx, false);
+    if (precision != AMRLBM_FP64 && !s.mp.C) {
+        const size_t NB = (size_t)ctx->prm.max_blks + 1;
+        cudaError_t e = cudaSuccess;
+#define ALM(field, T, n)                                                   \
+        s.mp.field = dalloc<T>(ctx, (n), &e);                              \
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc mp." #field);
+        ALM(C, float, NB * s.cplane);
+        ALM(P, float, NB * s.pplane);
+        ALM(Ux, float, NB * s.pplane);
+        ALM(Uy, float, NB * s.pplane);
+        ALM(A1h, float, NB * s.aplane);
+        ALM(A1g, float, NB * s.aplane);
+        ALM(B1h, float, NB * s.bplane);
+        ALM(B1g, float, NB * s.bplane);
+        ALM(Adh, unsigned short, NB * 9 * s.aplane);
+        ALM(Adg, unsigned short, NB * 9 * s.aplane);
+        ALM(Bdh, unsigned short, NB * 9 * s.bplane);
+        ALM(Bdg, unsigned short, NB * 9 * s.bplane);
+#undef ALM
+    }
+    s.mp.fmt = precision;
+    // FP16 keeps the deviations in its normal range with power-of-two scales
+    // (exact); BF16 has FP32's exponent range and needs none
+    s.mp.sh = precision == AMRLBM_FP16 ? 16.f : 1.f;
+    s.mp.sg = precision == AMRLBM_FP16 ? 4096.f : 1.f;
+    s.mp.ish = 1.f / s.mp.sh;
+    s.mp.isg = 1.f / s.mp.sg;
+    s.mp.ph = to_physf(s.ph);
+    ctx->mp_stale = true;
+    ctx->fp64_stale = false;
+    drop_graphs(ctx);
+    launch_mp_prepare(s, ctx->lc);
+    return sync_check(ctx);
+}
+
+int amrlbm_get_fill_order(amrlbm_ctx* ctx, int32_t needs_order[3]) {
+    if (!ctx || !needs_order) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    int f[NQUEUES];
+    CK(cudaMemcpy(f, ctx->s.fillinfo, sizeof(f), cudaMemcpyDeviceToHost));
+    needs_order[0] = f[Q_FILLC] != 0;
+    needs_order[1] = f[Q_FILLC1] != 0;
+    needs_order[2] = f[Q_FILLHG] != 0;
     return AMRLBM_OK;
 }
 
@@ -595,6 +731,7 @@ int amrlbm_set_topology(amrlbm_ctx* ctx, int32_t nblks, const int32_t* level, co
         n_free > ctx->s.fl_cap - 1 || !level || !dx || !bi || !bj || !parent || !child ||
         !nbr_owner || !nbr_slot || !flags)
         return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, true);
     DevState& s = ctx->s;
     const size_t NB = (size_t)ctx->prm.max_blks + 1;
     std::vector<int> lv(NB, -1), d(NB, 0), I(NB, 0), J(NB, 0), pa(NB, -1), ch(4 * NB, 0),
@@ -741,6 +878,7 @@ int amrlbm_upload_fields(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, const d
                          const double* Uy) {
     if (!ctx || n < 0 || (n > 0 && !ids)) return AMRLBM_ERR_ARG;
     if (n == 0) return AMRLBM_OK;
+    ensure_fp64(ctx, true);
     int r = upload_blocks(ctx, n, ids, h, g, C, P, Ux, Uy);
     if (r) return r;
     ctx->tail_done = true;
@@ -751,6 +889,7 @@ int amrlbm_download_fields(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, doubl
                            double* C, double* P, double* Ux, double* Uy) {
     if (!ctx || n < 0 || (n > 0 && !ids)) return AMRLBM_ERR_ARG;
     if (n == 0) return AMRLBM_OK;
+    ensure_fp64(ctx, false);
     for (int i = 0; i < n; ++i)
         if (ids[i] < 1 || ids[i] > ctx->prm.max_blks) return AMRLBM_ERR_ARG;
     double* dst[6] = {h, g, C, P, Ux, Uy};
@@ -796,17 +935,25 @@ int amrlbm_get_block_error(amrlbm_ctx* ctx, double* err) {
 // driver does; P, U, h and g are derived from it on the device.
 int amrlbm_init_fields(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, true);
     CK(cudaStreamSynchronize(ctx->st));
     std::vector<int> leaves;
     HostTopo t;
     if (int r = get_leaves_host(ctx, leaves, t)) return r;
     const int nx = ctx->prm.nx, ny = ctx->prm.ny;
-    const double R = ctx->prm.radius, X0 = ctx->prm.xc, Y0 = ctx->prm.yc, W = ctx->s.ph.W;
     const size_t cs = (size_t)(nx + 4) * (ny + 4);
+    std::vector<int> inst;  // batches: the instance of every block
+    if (ctx->s.n_inst) {
+        inst.resize(t.dx.size());
+        CK(cudaMemcpy(inst.data(), ctx->s.inst, inst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    }
     std::vector<double> C(leaves.size() * cs);
     for (size_t m = 0; m < leaves.size(); ++m) {
         const int n = leaves[m];
         const int dx = t.dx[n];
+        const amrlbm_instance* bi = ctx->s.n_inst ? &ctx->insts[inst[n]] : nullptr;
+        const double R = bi ? bi->radius : ctx->prm.radius, X0 = bi ? bi->xc : ctx->prm.xc,
+                     Y0 = bi ? bi->yc : ctx->prm.yc, W = bi ? bi->w : ctx->s.ph.W;
         double* c = C.data() + m * cs;
         for (int j = -1; j <= ny + 2; ++j)
             for (int i = -1; i <= nx + 2; ++i) {
@@ -821,15 +968,20 @@ int amrlbm_init_fields(amrlbm_ctx* ctx) {
                                   C.data(), nullptr, nullptr, nullptr))
             return r;
     }
-    launch_init_fields(ctx->s, ctx->lc, ctx->st, R, ctx->prm.hydrostatic_start, Y0);
+    launch_init_fields(ctx->s, ctx->lc, ctx->st, ctx->prm.radius, ctx->prm.hydrostatic_start,
+                       ctx->prm.yc);
     ctx->tail_done = true;
     return sync_check(ctx);
 }
 
 // AMR_LBM_Rising_Bubble (AMR_Rising_2D_OMP.f90:49-67) with the base grid
 // generalised to nbx x nby blocks (periodic in x, walls in y).
+int init_batch(amrlbm_ctx* ctx);
+
 int amrlbm_init_rising_bubble(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, true);
+    if (ctx->s.n_inst) return init_batch(ctx);
     const amrlbm_params& p = ctx->prm;
     const int nbx = p.nbx, nby = p.nby, nb = nbx * nby;
     // Initialize_Base_Block + Fix_Initial_Neighbors_3Blocks (:79-138)
@@ -903,12 +1055,14 @@ int amrlbm_min_max_levels(amrlbm_ctx* ctx, int32_t* lmin, int32_t* lmax) {
 
 int amrlbm_fill_ghost_c2(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, true);
     launch_fill_c(ctx->s, ctx->lc, ctx->st, 2, CONS_NONE);
     return sync_check(ctx);
 }
 
 int amrlbm_phase_field_step(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, true);
     launch_collide(ctx->s, ctx->lc, ctx->st);
     launch_fill_hg_stream(ctx->s, ctx->lc, ctx->st);
     ctx->tail_done = false;
@@ -917,18 +1071,21 @@ int amrlbm_phase_field_step(amrlbm_ctx* ctx) {
 
 int amrlbm_macro_h(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, true);
     launch_macro_h(ctx->s, ctx->lc, ctx->st);
     return sync_check(ctx);
 }
 
 int amrlbm_fill_ghost_c(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, true);
     launch_fill_c(ctx->s, ctx->lc, ctx->st, 1, CONS_NONE);
     return sync_check(ctx);
 }
 
 int amrlbm_macro_g(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, true);
     launch_macro_g(ctx->s, ctx->lc, ctx->st);
     ctx->tail_done = true;
     return sync_check(ctx);
@@ -936,6 +1093,7 @@ int amrlbm_macro_g(amrlbm_ctx* ctx) {
 
 int amrlbm_regrid(amrlbm_ctx* ctx, double refin_tol, double deref_tol) {
     if (!ctx) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, true);
     enqueue_regrid(ctx, refin_tol, deref_tol, true, false);
     ctx->tail_done = true;
     return sync_check(ctx);
@@ -945,6 +1103,11 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
     if (!ctx || nsteps < 0) return AMRLBM_ERR_ARG;
     if (nsteps == 0) return AMRLBM_OK;
     const int R = ctx->prm.regrid_every;
+    if (ctx->s.mp.fmt) {
+        if (ctx->mp_stale) launch_mp_convert(ctx->s, ctx->lc, ctx->st, 0, 1);
+        ctx->mp_stale = false;
+        ctx->fp64_stale = true;
+    }
     launch_minmax(ctx->s, ctx->st);  // Determine_Min_Max_Levels
     int done = 0;
     while (done < nsteps) {
@@ -1002,6 +1165,7 @@ int amrlbm_sync(amrlbm_ctx* ctx) {
 
 int amrlbm_diag(amrlbm_ctx* ctx, double out[8]) {
     if (!ctx || !out) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, false);
     launch_diag(ctx->s, ctx->st, ctx->d_diag);
     double o[9];
     CK(cudaMemcpyAsync(o, ctx->d_diag, 9 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
@@ -1013,6 +1177,7 @@ int amrlbm_diag(amrlbm_ctx* ctx, double out[8]) {
 
 int amrlbm_write_tecplot(amrlbm_ctx* ctx, const char* path, int32_t t) {
     if (!ctx || !path) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, false);
     if (int r = sync_check(ctx)) return r;
     const Counters c = read_counters(ctx);
     const int nx = ctx->prm.nx, ny = ctx->prm.ny, nl = c.nleaf;
@@ -1245,6 +1410,7 @@ extern "C" int amrlbm_download_fields_noalloc(amrlbm_ctx* ctx, int32_t n, const 
     if (n > AMRLBM_NOALLOC_MAX_BLOCKS || used > (size_t)AMRLBM_NOALLOC_STAGE_DOUBLES)
         return AMRLBM_ERR_CAPACITY;
     if (used == 0) return AMRLBM_OK;
+    ensure_fp64(ctx, false);  // kernels only: no allocation
     // the device that holds the context's pool, current for this call
     cudaPointerAttributes pa;
     if (cudaPointerGetAttributes(&pa, ctx->s.C) != cudaSuccess) return AMRLBM_ERR_CUDA;
@@ -1286,3 +1452,248 @@ extern "C" int amrlbm_download_fields_noalloc(amrlbm_ctx* ctx, int32_t n, const 
     if (prev != pa.device) cudaSetDevice(prev);
     return rc;
 }
+
+// ===========================================================================
+// Batched instances: many independent rising bubbles in one pool, advanced
+// by the same launches. No counterpart in the reference, which runs one
+// bubble per process.
+namespace {
+
+// the reference's parameter derivation (Set_Rising_Bubble_Parameters) for
+// one instance on top of the batch's params
+amrlbm_params instance_params(const amrlbm_params& base, const amrlbm_instance& in) {
+    amrlbm_params q = base;
+    q.nbx = in.nbx;
+    q.nby = in.nby;
+    q.dx0 = in.dx0;
+    q.min_levels = 0;
+    q.max_levels = in.max_levels;
+    q.rho_l = in.rho_l;
+    q.rho_h = in.rho_h;
+    q.visc_ratio = in.visc_ratio;
+    q.bo = in.bo;
+    q.ar = in.ar;
+    q.gy = in.gy;
+    q.w = in.w;
+    q.m0 = in.m0;
+    q.radius = in.radius;
+    q.xc = in.xc;
+    q.yc = in.yc;
+    q.hydrostatic_start = in.hydrostatic_start;
+    return q;
+}
+
+int set_active(amrlbm_ctx* ctx, int round) {
+    std::vector<unsigned char> a(ctx->insts.size());
+    for (size_t i = 0; i < a.size(); ++i) a[i] = (round < 0 || round < ctx->insts[i].max_levels) ? 1 : 0;
+    CK(cudaMemcpy(ctx->d_active, a.data(), a.size(), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+}  // namespace
+
+// AMR_LBM_Rising_Bubble (AMR_Rising_2D_OMP.f90:49-67) for every instance of
+// a batch: each instance's base blocks (periodic in x, walls in y) take
+// consecutive ids, then the start-up rounds of Refine_Derefine_Mesh and the
+// analytic bubble; an instance takes part in as many rounds as it has levels,
+// so it goes through exactly the rounds of its own start-up.
+int init_batch(amrlbm_ctx* ctx) {
+    const auto& I = ctx->insts;
+    int nb = 0, maxlv = 0;
+    for (const auto& in : I) {
+        nb += in.nbx * in.nby;
+        maxlv = std::max(maxlv, in.max_levels);
+    }
+    if (nb > ctx->prm.max_blks) return fail(ctx, AMRLBM_ERR_POOL_FULL, "base blocks exceed max_blks");
+    std::vector<int> level(nb, 0), dx(nb), bi(nb), bj(nb), parent(nb, -1), child(4 * nb),
+        own(8 * nb), slot(8 * nb, 0), inst(ctx->prm.max_blks + 1, -1);
+    std::vector<uint8_t> flags(nb, AMRLBM_F_LEAF | AMRLBM_F_ALLOC);
+    int base = 0;
+    for (size_t k = 0; k < I.size(); ++k) {
+        const int nbx = I[k].nbx, nby = I[k].nby;
+        auto id = [&](int x, int y) { return base + 1 + ((x % nbx + nbx) % nbx) + nbx * y; };
+        for (int y = 0; y < nby; ++y)
+            for (int x = 0; x < nbx; ++x) {
+                const int n = id(x, y), i = n - 1;
+                dx[i] = I[k].dx0;
+                bi[i] = x;
+                bj[i] = y;
+                inst[n] = (int)k;
+                for (int c = 0; c < 4; ++c) child[4 * i + c] = n;
+                const bool lo = y > 0, hi = y < nby - 1;
+                const int v[8] = {id(x - 1, y),  id(x + 1, y),
+                                  lo ? id(x, y - 1) : -3,     hi ? id(x, y + 1) : -4,
+                                  lo ? id(x - 1, y - 1) : -5, hi ? id(x - 1, y + 1) : -6,
+                                  lo ? id(x + 1, y - 1) : -7, hi ? id(x + 1, y + 1) : -8};
+                for (int c = 0; c < 8; ++c) own[8 * i + c] = v[c];
+            }
+        base += nbx * nby;
+    }
+    CK(cudaMemcpy(ctx->s.inst, inst.data(), inst.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (int r = amrlbm_set_topology(ctx, nb, level.data(), dx.data(), bi.data(), bj.data(),
+                                    parent.data(), child.data(), own.data(), slot.data(),
+                                    flags.data(), 0, nullptr, 0))
+        return r;
+    {
+        std::vector<int> ids(nb);
+        for (int n = 1; n <= nb; ++n) ids[n - 1] = n;
+        const size_t hs = (size_t)9 * (ctx->prm.nx + 2) * (ctx->prm.ny + 2),
+                     cs = (size_t)(ctx->prm.nx + 4) * (ctx->prm.ny + 4),
+                     ps = (size_t)ctx->prm.nx * ctx->prm.ny;
+        std::vector<double> zh(nb * hs, 0.0), zc(nb * cs, 0.0), zp(nb * ps, 0.0);
+        if (int r = upload_blocks(ctx, nb, ids.data(), zh.data(), zh.data(), zc.data(), zp.data(),
+                                  zp.data(), zp.data()))
+            return r;
+    }
+    int lmax = 0;
+    if (int r = set_level_counters(ctx, 0, lmax)) return r;
+    if (int r = amrlbm_init_fields(ctx)) return r;
+    for (int round = 0; lmax < maxlv; ++round) {
+        if (int r = set_active(ctx, round)) return r;
+        if (int r = amrlbm_regrid(ctx, ctx->prm.refin_tol, ctx->prm.deref_tol)) return r;
+        if (int r = amrlbm_init_fields(ctx)) return r;
+        lmax = lmax + 1;
+        if (int r = set_level_counters(ctx, 0, lmax)) return r;
+    }
+    if (int r = set_active(ctx, -1)) return r;
+    ctx->stepcount = 0;
+    ctx->tail_done = true;
+    return AMRLBM_OK;
+}
+
+extern "C" {
+
+int amrlbm_create_batch(const amrlbm_params* p, int32_t n_inst, const amrlbm_instance* inst,
+                        amrlbm_ctx** out) {
+    if (!p || !out || n_inst < 1 || !inst) return AMRLBM_ERR_ARG;
+    *out = nullptr;
+    if (p->nx != p->ny || (p->nx != 8 && p->nx != 16)) return AMRLBM_ERR_ARG;
+    amrlbm_params q = *p;
+    q.nbx = q.nby = 1;
+    q.min_levels = 0;
+    q.dx0 = 1;
+    q.max_levels = 0;
+    long long nb = 0;
+    for (int i = 0; i < n_inst; ++i) {
+        const amrlbm_instance& in = inst[i];
+        if (in.nbx < 1 || in.nby < 1 || in.dx0 < 1 || (in.dx0 & (in.dx0 - 1)) || in.max_levels < 0 ||
+            (in.dx0 >> in.max_levels) < 1 || in.hydrostatic_start < 0 || in.hydrostatic_start > 1)
+            return AMRLBM_ERR_ARG;
+        q.dx0 = std::max(q.dx0, in.dx0);
+        q.max_levels = std::max(q.max_levels, in.max_levels);
+        nb += (long long)in.nbx * in.nby;
+    }
+    if (nb > p->max_blks) return AMRLBM_ERR_ARG;
+    // amrlbm_create checks dx0 >> max_levels >= 1 for the largest of each
+    while ((q.dx0 >> q.max_levels) < 1) q.dx0 *= 2;
+    if (int r = amrlbm_create(&q, out)) return r;
+    amrlbm_ctx* ctx = *out;
+    DevState& s = ctx->s;
+    const size_t NB = (size_t)q.max_blks + 1;
+    std::vector<PhysD> ph(n_inst);
+    std::vector<PhysF> pf(n_inst);
+    std::vector<int> mlv(n_inst);
+    std::vector<double> geo(4 * (size_t)n_inst);
+    for (int i = 0; i < n_inst; ++i) {
+        const amrlbm_params ip = instance_params(q, inst[i]);
+        amrlbm_physics phys;
+        amrlbm_derive_physics(&ip, &phys);
+        ph[i] = to_physd(phys);
+        pf[i] = to_physf(ph[i]);
+        mlv[i] = inst[i].max_levels;
+        geo[4 * i] = inst[i].radius;
+        geo[4 * i + 1] = inst[i].xc;
+        geo[4 * i + 2] = inst[i].yc;
+        geo[4 * i + 3] = inst[i].hydrostatic_start;
+    }
+    cudaError_t e = cudaSuccess;
+    int* d_inst = dalloc<int>(ctx, NB, &e);
+    PhysD* d_ph = e == cudaSuccess ? dalloc<PhysD>(ctx, n_inst, &e) : nullptr;
+    PhysF* d_pf = e == cudaSuccess ? dalloc<PhysF>(ctx, n_inst, &e) : nullptr;
+    int* d_mlv = e == cudaSuccess ? dalloc<int>(ctx, n_inst, &e) : nullptr;
+    double* d_geo = e == cudaSuccess ? dalloc<double>(ctx, 4 * (size_t)n_inst, &e) : nullptr;
+    unsigned char* d_act = e == cudaSuccess ? dalloc<unsigned char>(ctx, n_inst, &e) : nullptr;
+    if (e == cudaSuccess) e = cudaMemcpy(d_ph, ph.data(), n_inst * sizeof(PhysD), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_pf, pf.data(), n_inst * sizeof(PhysF), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_mlv, mlv.data(), n_inst * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_geo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_act, 1, n_inst);
+    if (e != cudaSuccess) {
+        const int r = cuda_fail(ctx, e, "batch tables");
+        amrlbm_destroy(ctx);
+        *out = nullptr;
+        return r;
+    }
+    s.n_inst = n_inst;
+    s.inst = d_inst;
+    s.phys = d_ph;
+    s.mp.phys = d_pf;
+    s.inst_maxlv = d_mlv;
+    s.inst_geo = d_geo;
+    s.inst_active = d_act;
+    ctx->d_active = d_act;
+    ctx->insts.assign(inst, inst + n_inst);
+    return AMRLBM_OK;
+}
+
+int amrlbm_get_instances(amrlbm_ctx* ctx, int32_t* inst) {
+    if (!ctx || !inst) return AMRLBM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->st));
+    const Counters c = read_counters(ctx);
+    if (!ctx->s.n_inst) {
+        for (int n = 1; n <= c.nblks; ++n) inst[n - 1] = 0;
+        return AMRLBM_OK;
+    }
+    CK(cudaMemcpy(inst, ctx->s.inst + 1, (size_t)c.nblks * sizeof(int), cudaMemcpyDeviceToHost));
+    return AMRLBM_OK;
+}
+
+int amrlbm_diag_instances(amrlbm_ctx* ctx, double* out) {
+    if (!ctx || !out) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, false);
+    const int ni = ctx->s.n_inst ? ctx->s.n_inst : 1;
+    launch_diag(ctx->s, ctx->st, ctx->d_diag);  // per-leaf partials after the first 9
+    if (int r = sync_check(ctx)) return r;
+    const Counters c = read_counters(ctx);
+    std::vector<double> part(9 * (size_t)c.nleaf);
+    std::vector<int> leaves(c.nleaf), inst(ctx->prm.max_blks + 1, 0);
+    if (c.nleaf) {
+        CK(cudaMemcpy(part.data(), ctx->d_diag + 9, part.size() * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(leaves.data(), ctx->s.leaf, c.nleaf * sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    if (ctx->s.n_inst)
+        CK(cudaMemcpy(inst.data(), ctx->s.inst, inst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    // the fixed summation order of amrlbm_diag, per instance (leaf order)
+    std::vector<double> acc(9 * (size_t)ni, 0.0);
+    for (int i = 0; i < ni; ++i) {
+        acc[9 * i + 1] = 10.0;
+        acc[9 * i + 2] = -10.0;
+    }
+    for (int m = 0; m < c.nleaf; ++m) {
+        double* a = &acc[9 * (size_t)inst[leaves[m]]];
+        const double* v = &part[9 * (size_t)m];
+        a[0] = a[0] + v[0];
+        a[1] = std::fmin(a[1], v[1]);
+        a[2] = std::fmax(a[2], v[2]);
+        a[3] = std::fmax(a[3], v[3]);
+        for (int k = 4; k < 9; ++k) a[k] = a[k] + v[k];
+    }
+    bool bad = false;
+    for (int i = 0; i < ni; ++i) {
+        const double* a = &acc[9 * (size_t)i];
+        double* o = out + 8 * (size_t)i;
+        o[0] = a[0];
+        o[1] = a[1];
+        o[2] = a[2];
+        o[3] = a[3];
+        o[4] = a[4];
+        o[5] = a[5] / a[4];
+        o[6] = a[6] / a[4];
+        o[7] = a[7];
+        if (a[8] != 0.0) bad = true;
+    }
+    if (bad) return fail(ctx, AMRLBM_ERR_NAN, "non-finite C or Uy in a leaf");
+    return AMRLBM_OK;
+}
+
+}  // extern "C"

@@ -60,6 +60,30 @@ enum { NBI_STRIDE = 64, PLAN_INTS = 10 };
 //   C      : order parameter with both ghost rings, [blk][y+1][col],
 //            col = x+3 (x = -1..nx+2), y = -1..ny+2
 //   P,Ux,Uy: [blk][y][x], x,y = 1..nx,ny
+// Physical constants of the mixed-precision kernels (FP32 copies of PhysD's)
+struct PhysF {
+    float W, iW, Beta4, kappa, M0, wc, omwc, Rhol, Rhoh, dRho, dRho3, dRho6, Gy;
+    float itau_d, itaul, taul5, tauh5;
+};
+
+// Mixed-precision state (amrlbm_set_precision): the same element layouts as
+// the FP64 pools, so the fill plans' source offsets index them unchanged.
+// A population f_q of a cell is stored as its rest population f_1 in FP32
+// (A1 / B1, one plane per block) and, for q = 2..9, the deviation
+// (f_q - (w_q/w_1) f_1) * scale in 16 bits (Ad / Bd, the 9-plane layout of
+// Ah / Bh, plane 1 unused); w_q/w_1 is 1/4 or 1/16, and the scales are powers
+// of two, so encoding adds only the 16-bit rounding. C (with both ghost
+// rings), P, Ux, Uy are FP32.
+struct MpState {
+    int fmt;                  // 0 off, 1 FP16, 2 BF16
+    float sh, sg, ish, isg;   // deviation scales of h and g, and their inverses
+    float *C, *P, *Ux, *Uy;
+    float *A1h, *A1g, *B1h, *B1g;
+    unsigned short *Adh, *Adg, *Bdh, *Bdg;
+    PhysF ph;
+    const PhysF* phys;  // batched instances: per instance (else ph)
+};
+
 // default bound of a flag wait of the level-ordered fills: iterations of
 // about 64 ns, about a second in all
 constexpr int AMR_SPIN_LIMIT = 20000000;
@@ -95,7 +119,31 @@ struct DevState {
     int spin_limit;   // iterations of a flag wait of the level-ordered fills
     int hold_flag;    // test hook: this block's ring flag is never raised (0: none)
     PhysD ph;
+    MpState mp;
+    // batched instances (amrlbm_create_batch): disconnected quadtrees in one
+    // pool, each with its own physics, bubble and number of levels; n_inst 0:
+    // one mesh, the params' (ph, max_levels)
+    int n_inst;
+    int* inst;             // instance of each block id
+    const PhysD* phys;     // per instance
+    const int* inst_maxlv; // maxLevels per instance
+    const double* inst_geo;  // per instance: radius, xc, yc, hydrostatic start (0/1)
+    const unsigned char* inst_active;  // per instance: regrids flag its blocks (start-up rounds)
 };
+
+// physics of block n's instance; BATCH: a compile-time choice, so the
+// one-mesh kernels keep reading the launch's constant parameter
+template <bool BATCH>
+__device__ __forceinline__ const PhysD& phys_of(const DevState& s, int n) {
+    if (BATCH) return s.phys[s.inst[n]];
+    return s.ph;
+}
+__device__ __forceinline__ const PhysD& phys_any(const DevState& s, int n) {
+    return s.n_inst ? s.phys[s.inst[n]] : s.ph;
+}
+__device__ __forceinline__ int maxlv_of(const DevState& s, int n) {
+    return s.n_inst ? s.inst_maxlv[s.inst[n]] : s.max_levels;
+}
 
 // ---------------------------------------------------------------------------
 // indexing

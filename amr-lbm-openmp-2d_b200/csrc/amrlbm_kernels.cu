@@ -38,13 +38,17 @@ __device__ __forceinline__ void ring1_xy(int r, int nx, int ny, int& x, int& y) 
 // Initialize_AMR_Rising_Bubble (AMR_Rising_2D_OMP.f90:186-226) given C
 // hydro != 0: P also carries the light phase's hydrostatic head about the
 // bubble centre y0, Gy*(Rhoh-Rhol)*(1-C)*(y-y0) (amrlbm_params.hydrostatic_start)
-__global__ void __launch_bounds__(256) k_init_fields(DevState s, double R, int hydro, double Y0) {
+__global__ void __launch_bounds__(256) k_init_fields(DevState s, double R0, int hydro0, double Y00) {
     extern __shared__ double T[];
     const int nleaf = s.cnt->nleaf, nx = s.nx, ny = s.ny, TW = nx + 4;
-    const PhysD& ph = s.ph;
-    const double dRho3 = (ph.Rhoh - ph.Rhol) / 3.0;
     for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
         const int n = s.leaf[m];
+        // the block's instance (batches) or the params' bubble
+        const PhysD& ph = phys_any(s, n);
+        const double* geo = s.n_inst ? s.inst_geo + 4 * s.inst[n] : nullptr;
+        const double R = geo ? geo[0] : R0, Y0 = geo ? geo[2] : Y00;
+        const int hydro = geo ? (geo[3] != 0.0) : hydro0;
+        const double dRho3 = (ph.Rhoh - ph.Rhol) / 3.0;
         const int dx = s.dx[n];
         load_tile(s, n, T);
         for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
@@ -163,10 +167,10 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_flags(DevState s, 
     __syncthreads();
     for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
         uint8_t r = 0;
-        if (s.is_leaf[n]) {
+        if (s.is_leaf[n] && (!s.n_inst || s.inst_active[s.inst[n]])) {
             if (s.level[n] < s.min_levels)
                 r = 1;
-            else if (s.level[n] < s.max_levels && s.err[n] > refin_tol)
+            else if (s.level[n] < maxlv_of(s, n) && s.err[n] > refin_tol)
                 r = 1;
         }
         s.refin[n] = r;
@@ -191,7 +195,7 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_flags(DevState s, 
     }
     for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
         uint8_t d = 0;
-        if (s.has_leaf[n] && s.level[n] >= s.min_levels) {
+        if (s.has_leaf[n] && s.level[n] >= s.min_levels && (!s.n_inst || s.inst_active[s.inst[n]])) {
             const int c1 = s.child[4 * n];
             if (!(s.refin[c1] || s.refin[c1 + 1] || s.refin[c1 + 2] || s.refin[c1 + 3])) {
                 d = 1;
@@ -447,6 +451,7 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_topo(DevState s, i
                         const int N = c1 + I + 2 * J;
                         s.level[N] = L + 1;
                         s.dx[N] = s.dx[par] / 2;
+                        if (s.n_inst) s.inst[N] = s.inst[par];
                         s.bi[N] = 2 * s.bi[par] + I;
                         s.bj[N] = 2 * s.bj[par] + J;
                         s.parent[N] = par;
@@ -584,7 +589,7 @@ __global__ void __launch_bounds__(256) k_prolong(DevState s) {
                 double g[10];
                 for (int q = 1; q <= 9; ++q) g[q] = s.Bg[b_idx(s, ch, q, x, y)];
                 double P, Ux, Uy;
-                macro_g_cell(s.ph, dx, Cs, g, P, Ux, Uy);
+                macro_g_cell(phys_any(s, ch), dx, Cs, g, P, Ux, Uy);
                 s.P[p_idx(s, ch, x, y)] = P;
                 s.Ux[p_idx(s, ch, x, y)] = Ux;
                 s.Uy[p_idx(s, ch, x, y)] = Uy;
@@ -672,7 +677,7 @@ __global__ void k_diag_blocks(DevState s, double* part) {
         if (threadIdx.x == 0) {
             const int dx = s.dx[n];
             const double a = (double)(dx * dx);
-            const PhysD& ph = s.ph;
+            const PhysD& ph = phys_any(s, n);
             double mass = 0, rmin = 10, rmax = -10, umax = 0, vol = 0, ysum = 0, vsum = 0, phase = 0;
             bool finite = true;
             for (int j = 1; j <= ny; ++j)

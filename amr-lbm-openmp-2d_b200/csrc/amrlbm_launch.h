@@ -62,3 +62,19 @@ void count_launches(int n);
 // div_rn against IEEE division on n random operands (divisor 0: random)
 int selftest_division(unsigned long long n, unsigned long long seed, double divisor,
                       unsigned long long* mismatches);
+
+// mixed-precision time step (amrlbm_mixed.cu); s.mp.fmt != 0, nx = ny = 8 or 16.
+// read_pu: P, U of the state are in memory (else the collision evaluates
+// Macroscopic_Values_g_AMR); write_pu / write_ring: the last step of a call
+void launch_mp_collide(const DevState& s, const LaunchCfg& lc, cudaStream_t st, bool read_pu,
+                       int write_pu);
+void launch_mp_fill_hg_stream(const DevState& s, const LaunchCfg& lc, cudaStream_t st,
+                              int write_ring);
+void launch_mp_tail(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
+// occupancy queries and shared-memory opt-ins of the kernels above (outside
+// stream capture, once per block size and format)
+void launch_mp_prepare(const DevState& s, const LaunchCfg& lc);
+// mode: 0 every leaf, 1 derefined parents, 2 their children, 3 refined
+// parents, 4 their children; to_mp: FP64 -> mixed, else back
+void launch_mp_convert(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int mode,
+                       int to_mp);

@@ -121,6 +121,28 @@ int amrlbm_set_physics(amrlbm_ctx* ctx, const amrlbm_physics* phys);
  * the reference keeps commented out at :180. */
 enum { AMRLBM_G_MRT = 0, AMRLBM_G_BGK = 1 };
 int amrlbm_set_g_collision(amrlbm_ctx* ctx, int32_t model);
+/* Storage precision of amrlbm_step; no counterpart in the reference, which
+ * is FP64 throughout. AMRLBM_FP64 (the default) is the reference's
+ * arithmetic, bit for bit. AMRLBM_FP16 / AMRLBM_BF16: the populations h and g
+ * are stored in 16 bits as deviations (f_q - (w_q/w_1) f_1, the rest
+ * population f_1 kept in FP32), C, P, Ux, Uy in FP32, and collision, ghost-cell
+ * interpolation and streaming run in FP32; the regrid's restriction sums and
+ * the diagnostics stay FP64 (Restrict.f90:14-65 on FP64 copies of the blocks
+ * involved). Needs 8x8 or 16x16 blocks. The FP64 pool remains the state that
+ * every other entry point reads and writes: after mixed-precision steps the
+ * first such call converts the state back (rounded values), and the next
+ * amrlbm_step converts it forward again. Results follow the FP64 trajectory
+ * within the 16-bit rounding, not bit for bit. */
+enum { AMRLBM_FP64 = 0, AMRLBM_FP16 = 1, AMRLBM_BF16 = 2 };
+int amrlbm_set_precision(amrlbm_ctx* ctx, int32_t precision);
+/* Whether the current mesh's ghost fills need level order (1) or not (0):
+ * [0] Fill_Ghost_Cells_C2, [1] Fill_Ghost_Cells_C, [2] Fill_Ghost_Cells_hg.
+ * A fill needs it where a coarse-to-fine stencil reads a coarser
+ * neighbour's ghost cell that is itself coarse-to-fine or a wall cell (the
+ * reference's DO L = LevelMin, LevelMax loops, Fill_Ghost_Cells_C.f90:8-38);
+ * its kernels then take the leaves in level order with bounded waits. A
+ * performance diagnostic; no counterpart in the reference. */
+int amrlbm_get_fill_order(amrlbm_ctx* ctx, int32_t needs_order[3]);
 /* Failure-detection test hook; no counterpart in the reference, whose
  * OpenMP barriers cannot time out. The level-ordered fills (a level range
  * narrower than the leaves) order their items by per-block flags, and every
@@ -260,6 +282,34 @@ int64_t amrlbm_launch_count(const amrlbm_ctx* ctx);
 int amrlbm_selftest_division(uint64_t n, uint64_t seed, double divisor, uint64_t* mismatches);
 /* Writes a buffer larger than the L2 cache on the context's stream. */
 int amrlbm_flush_l2(amrlbm_ctx* ctx);
+
+/* ---- batched instances ----------------------------------------------------
+ * No counterpart in the reference, which runs one bubble per process. A batch
+ * holds many independent rising-bubble problems in one pool; every entry
+ * point above (amrlbm_step in FP64 or mixed precision, the transfers, the
+ * regrid) advances all of them in the same launches. Each instance has its own
+ * base grid (nbx x nby blocks of dx0 finest cells, periodic in x, walls in y),
+ * number of levels, physics (derived as Set_Rising_Bubble_Parameters,
+ * AMR_Rising_2D_OMP.f90:235-263, does for one) and bubble; block size, pool
+ * size, tolerances and regrid interval are the batch's (amrlbm_params, whose
+ * own physics and geometry fields are not used). Every instance's fields
+ * equal, bit for bit, those of the same problem run alone; its block ids are
+ * the pool's. amrlbm_init_rising_bubble starts every instance up
+ * (AMR_Rising_2D_OMP.f90:49-67), each with as many start-up regrid rounds as
+ * it has levels. 8x8 or 16x16 blocks. */
+typedef struct amrlbm_instance {
+    int32_t nbx, nby, dx0, max_levels;
+    double rho_l, rho_h, visc_ratio, bo, ar, gy, w, m0;
+    double radius, xc, yc;
+    int32_t hydrostatic_start;
+} amrlbm_instance;
+int amrlbm_create_batch(const amrlbm_params* p, int32_t n_inst, const amrlbm_instance* inst,
+                        amrlbm_ctx** out);
+/* inst[id-1] = instance (0-based) of blocks 1..Nblks (0 for one mesh). */
+int amrlbm_get_instances(amrlbm_ctx* ctx, int32_t* inst);
+/* amrlbm_diag per instance: out[8*i .. 8*i+7] as amrlbm_diag's out[0..7],
+ * each instance's sums in leaf-list order. */
+int amrlbm_diag_instances(amrlbm_ctx* ctx, double* out);
 
 /* ---- download without allocation ----------------------------------------
  * No counterpart in the reference, whose fields live in host memory.
