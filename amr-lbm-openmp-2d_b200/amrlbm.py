@@ -276,6 +276,7 @@ def load_library(path: str | None = None):
         "amrlbm_set_wait_test": (ct.c_int, [vp, ct.c_int32, ct.c_int32]),
         "amrlbm_set_precision": (ct.c_int, [vp, ct.c_int32]),
         "amrlbm_get_fill_order": (ct.c_int, [vp, i32p]),
+        "amrlbm_set_launch": (ct.c_int, [vp, ct.c_int32]),
         "amrlbm_create_batch": (ct.c_int, [ct.POINTER(Params), ct.c_int32, ct.POINTER(Instance),
                                            ct.POINTER(vp)]),
         "amrlbm_get_instances": (ct.c_int, [vp, i32p]),
@@ -424,6 +425,11 @@ class AmrLbm:
         if isinstance(precision, str):
             precision = {"fp64": FP64, "fp16": FP16, "bf16": BF16}[precision.lower()]
         self._check(self.lib.amrlbm_set_precision(self.ctx, int(precision)))
+
+    def set_launch(self, ctas_per_sm: int = 0):
+        """At most ctas_per_sm CTAs per SM for the mixed-precision kernels
+        (0: as many as fit; amrlbm_set_launch)."""
+        self._check(self.lib.amrlbm_set_launch(self.ctx, int(ctas_per_sm)))
 
     def fill_order(self):
         """Which ghost fills of the current mesh need level order
@@ -637,3 +643,64 @@ class AmrLbm:
 
     def device_bytes(self) -> int:
         return int(self.lib.amrlbm_device_bytes(self.ctx))
+
+
+# ---------------------------------------------------------------------------
+# Autotuner of the batched mixed-precision step: block size (8x8 or 16x16
+# cells, i.e. 2 or 8 warps per CTA) and CTAs per SM, timed on the batch
+# itself.
+
+def rescale_instances(instances, n_from: int, n_to: int):
+    """The same problems described in n_to x n_to blocks."""
+    out = []
+    for i in instances:
+        d = i.as_dict()
+        assert (i.nbx * n_from) % n_to == 0 and (i.nby * n_from) % n_to == 0
+        d["nbx"], d["nby"] = i.nbx * n_from // n_to, i.nby * n_from // n_to
+        out.append(Instance(**d))
+    return out
+
+
+def time_intervals(sim: "AmrLbm", intervals: int, inner: int) -> float:
+    """Leaf-cell updates per second (millions) over `intervals` regrid
+    intervals, device-timed with the L2 flushed before each."""
+    c0 = sim.profile_read(0)[2]
+    ms = 0.0
+    for _ in range(intervals):
+        sim.flush_l2()
+        sim.sync()
+        sim.timer_start()
+        sim.main_loop(inner)
+        ms += sim.timer_stop()
+    return (sim.profile_read(0)[2] - c0) / (ms / 1e3) / 1e6
+
+
+def autotune(instances, precision="fp16", block_sizes=(16, 8), ctas=(0, 1, 2, 3, 4),
+             n_from: int = 16, max_blks: int = 0, warmup: int = 2, intervals: int = 3,
+             regrid_every: int = 10):
+    """Times the batch of `instances` (given in n_from x n_from blocks) for
+    every block size and CTA-per-SM cap, returns (best, table): best =
+    {"block": n, "ctas_per_sm": c, "mlups": v}, table = list of those for
+    every candidate that ran."""
+    table = []
+    for n in block_sizes:
+        insts = rescale_instances(instances, n_from, n)
+        mb = max_blks or 4 * sum(i.nbx * i.nby for i in insts) + 4096
+        try:
+            sim = AmrLbm(batch_params(n=n, max_blks=mb, regrid_every=regrid_every),
+                         instances=insts)
+        except AmrLbmError:
+            continue
+        try:
+            sim.initialize_rising_bubble()
+            sim.set_precision(precision)
+            for c in ctas:
+                sim.set_launch(c)
+                for _ in range(warmup):
+                    sim.main_loop(regrid_every)
+                table.append({"block": n, "ctas_per_sm": c,
+                              "mlups": time_intervals(sim, intervals, regrid_every)})
+        finally:
+            sim.close()
+    best = max(table, key=lambda r: r["mlups"]) if table else None
+    return best, table

@@ -681,6 +681,13 @@ int amrlbm_set_precision(amrlbm_ctx* ctx, int32_t precision) {
     return sync_check(ctx);
 }
 
+int amrlbm_set_launch(amrlbm_ctx* ctx, int32_t ctas_per_sm) {
+    if (!ctx || ctas_per_sm < 0 || ctas_per_sm > 32) return AMRLBM_ERR_ARG;
+    ctx->lc.mp_ctas = ctas_per_sm;
+    drop_graphs(ctx);
+    return AMRLBM_OK;
+}
+
 int amrlbm_get_fill_order(amrlbm_ctx* ctx, int32_t needs_order[3]) {
     if (!ctx || !needs_order) return AMRLBM_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->st));

@@ -17,6 +17,7 @@ struct LaunchCfg {
     int num_sms;
     int grid_queue;     // CTAs of a level-ordered kernel
     int grid_leaves;    // CTAs of a grid-stride kernel over leaves
+    int mp_ctas;        // CTAs per SM of the mixed-precision kernels (0: as many as fit)
 };
 
 // write_ring: without level order, the consumer items write the ghost rings

@@ -1034,8 +1034,9 @@ int per_sm(K kern, int threads, size_t dyn) {
 template <class K>
 void grid_leaves_launch(K kern, const LaunchCfg& lc, int threads, size_t dyn, cudaStream_t st,
                         const DevState& s, int a, bool prepare = false) {
-    const int b = per_sm(kern, threads, dyn);
+    int b = per_sm(kern, threads, dyn);
     if (prepare) return;
+    if (lc.mp_ctas > 0 && lc.mp_ctas < b) b = lc.mp_ctas;
     kern<<<lc.num_sms * b, threads, dyn, st>>>(s, a);
     count_launches(1);
 }

@@ -29,6 +29,12 @@ device's state at the start of the timed region, runs the same regrid
 intervals on all host cores (its diagnostics must then equal the device's bit
 for bit) and goes on to a bounded sample; a second leg runs at 4 threads, the
 reference's OMP_NUM_THREADS (AMR_Rising_2D_OMP.f90:23).
+
+Beside the FP64 value: mixed_precision (the same workload with FP16 / BF16
+population storage, MLUPS), mixed_precision_error (the 64x128-base bubble in
+FP16 and BF16 against FP64 at steps 1000 / 2500 / 5000: rise velocity,
+centroid, mass), batched (the seeded batch of 256 uneven problems in one pool,
+block size and CTAs per SM chosen by amrlbm.autotune, FP64 and FP16 MLUPS).
 """
 from __future__ import annotations
 
@@ -64,6 +70,8 @@ def parse():
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision, error-report and batched legs")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--max-blks", type=int, default=0,
                     help="pool capacity (default: a fully refined tree); smaller pools "
@@ -302,6 +310,71 @@ def run_reference(args):
     return 0
 
 
+def mixed_error_report(checkpoints=(1000, 2500, 5000)):
+    """The mixed-precision configuration's error report: the 64x128-base,
+    density-ratio-10 bubble run in FP64, FP16 and BF16 storage; rise velocity,
+    centroid and mass of each against FP64 at the checkpoints."""
+    import amrlbm
+    p = amrlbm.workload_small()
+    runs = {}
+    for prec in ("fp64", "fp16", "bf16"):
+        g = amrlbm.AmrLbm(p)
+        g.initialize_rising_bubble()
+        g.set_precision(prec)
+        done, out = 0, {}
+        for c in checkpoints:
+            g.main_loop(c - done)
+            done = c
+            out[c] = g.output()
+        g.close()
+        runs[prec] = out
+    rep = {}
+    for prec in ("fp16", "bf16"):
+        rows = {}
+        for c in checkpoints:
+            a, r = runs[prec][c], runs["fp64"][c]
+            check_state(a, f"{prec} run at step {c}")
+            rows[str(c)] = {
+                "rise_velocity_rel_err": abs(a["rise_velocity"] - r["rise_velocity"]) / abs(r["rise_velocity"]),
+                "centroid_err_cells": abs(a["y_centroid"] - r["y_centroid"]),
+                "mass_rel_err": abs(a["mass"] - r["mass"]) / r["mass"]}
+        rep[prec] = rows
+    rep["workload"] = "rising_bubble_base64x128_blocks16_L2_R32 (density ratio 10)"
+    rep["bounds"] = {"rise_velocity_rel_err": 0.01, "mass_rel_err": 1e-6}
+    return rep
+
+
+def batched_leg(count=256, tune_count=32, intervals=3):
+    """Batched uneven instances: the seeded 256-problem batch, block size and
+    CTAs per SM picked by amrlbm.autotune on its first tune_count problems,
+    then the whole batch timed in FP64 and in FP16."""
+    import amrlbm
+    insts = amrlbm.batch_instances(count)
+    best, table = amrlbm.autotune(insts[:tune_count], "fp16", intervals=1, warmup=1)
+    n = best["block"] if best else 16
+    run = amrlbm.rescale_instances(insts, 16, n)
+    g = amrlbm.AmrLbm(amrlbm.batch_params(n=n, max_blks=400000), instances=run)
+    g.initialize_rising_bubble()
+    c = g.counts()
+    res = {"instances": count, "block": f"{n}x{n}", "leaves": c["nleaf"],
+           "leaf_cells": c["nleaf"] * n * n, "autotune": {"best": best, "table": table}}
+    for _ in range(2):
+        g.main_loop(10)
+    res["fp64_mlups"] = amrlbm.time_intervals(g, intervals, 10)
+    g.set_precision("fp16")
+    g.set_launch(best["ctas_per_sm"] if best else 0)
+    for _ in range(2):
+        g.main_loop(10)
+    res["fp16_mlups"] = amrlbm.time_intervals(g, intervals, 10)
+    d = g.output_instances()
+    bad = [i for i, x in enumerate(d) if not (x["u_max"] < U_BOUND and x["rho_min"] > 0)]
+    if bad:
+        raise RuntimeError(f"batched instances {bad[:8]} not physical")
+    g.close()
+    res["fp16_vs_fp64_batched"] = res["fp16_mlups"] / res["fp64_mlups"]
+    return res
+
+
 def run_own(args):
     world, rank, local = dist_setup("nccl")
     import amrlbm
@@ -417,6 +490,17 @@ def run_own(args):
                "h2d_bytes_per_step": int(h2d / args.steps),
                "d2h_bytes_per_step": int(d2h / args.steps)}
 
+    # ---- the same workload with mixed-precision storage (the state goes on)
+    mixed = {}
+    if not args.no_mixed:
+        for prec in ("fp16", "bf16"):
+            gpu.set_precision(prec)
+            for _ in range(2):
+                gpu.main_loop(inner)
+            mixed[prec] = {"mlups": amrlbm.time_intervals(gpu, args.steps, inner)}
+            check_state(gpu.output(), f"{prec} leg")
+        gpu.set_precision("fp64")
+        mixed["fp64_mlups"] = value
     diag = gpu.output()
     if rank != 0:
         gpu.close()
@@ -463,6 +547,10 @@ def run_own(args):
                 "sample": f"the next {chunks4} x {inner} time steps ({el4:.1f} s) at 4 threads, "
                           f"the reference's OMP_NUM_THREADS"}
         orc.close()
+    mixed_err = batched = None
+    if not args.no_mixed:
+        mixed_err = mixed_error_report()
+        batched = batched_leg()
     line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -471,6 +559,8 @@ def run_own(args):
             "roofline": roofline, "cpu_baseline": cpu, "cpu_baseline_4_threads": cpu4,
             "e2e": e2e, "clocks": clk,
             "gpu_launches": int(launches), "kernels": kernels,
+            "mixed_precision": mixed or None, "mixed_precision_error": mixed_err,
+            "batched": batched,
             "leaf_cells_per_step": updates / (args.steps * inner),
             "diagnostics": {k: diag[k] for k in ("mass", "y_centroid", "rise_velocity")}}
     print(json.dumps(line), flush=True)

@@ -135,6 +135,11 @@ int amrlbm_set_g_collision(amrlbm_ctx* ctx, int32_t model);
  * within the 16-bit rounding, not bit for bit. */
 enum { AMRLBM_FP64 = 0, AMRLBM_FP16 = 1, AMRLBM_BF16 = 2 };
 int amrlbm_set_precision(amrlbm_ctx* ctx, int32_t precision);
+/* Launch shape of the mixed-precision kernels (one CTA of nx*ny threads per
+ * leaf item, persistent over the items): at most ctas_per_sm CTAs on each SM,
+ * 0 (the default) as many as fit. A tuning knob (amrlbm.autotune); results do
+ * not depend on it. */
+int amrlbm_set_launch(amrlbm_ctx* ctx, int32_t ctas_per_sm);
 /* Whether the current mesh's ghost fills need level order (1) or not (0):
  * [0] Fill_Ghost_Cells_C2, [1] Fill_Ghost_Cells_C, [2] Fill_Ghost_Cells_hg.
  * A fill needs it where a coarse-to-fine stencil reads a coarser
