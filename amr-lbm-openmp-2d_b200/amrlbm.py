@@ -264,6 +264,7 @@ def load_library(path: str | None = None):
     lib = ct.CDLL(p)
     i32p = ct.POINTER(ct.c_int32)
     dp = ct.POINTER(ct.c_double)
+    fp = ct.POINTER(ct.c_float)
     u8p = ct.POINTER(ct.c_uint8)
     vp = ct.c_void_p
     sig = {
@@ -277,6 +278,20 @@ def load_library(path: str | None = None):
         "amrlbm_set_precision": (ct.c_int, [vp, ct.c_int32]),
         "amrlbm_get_fill_order": (ct.c_int, [vp, i32p]),
         "amrlbm_set_launch": (ct.c_int, [vp, ct.c_int32]),
+        "amrlbm_net_create": (ct.c_int, [ct.c_uint64, ct.c_int32, ct.POINTER(vp)]),
+        "amrlbm_net_destroy": (ct.c_int, [vp]),
+        "amrlbm_net_param_count": (ct.c_int32, []),
+        "amrlbm_net_last_error": (ct.c_char_p, [vp]),
+        "amrlbm_net_get": (ct.c_int, [vp, fp]),
+        "amrlbm_net_set": (ct.c_int, [vp, fp]),
+        "amrlbm_net_forward": (ct.c_int, [vp, ct.c_int32, fp, fp]),
+        "amrlbm_net_gradient": (ct.c_int, [vp, ct.c_int32, fp, fp, ct.c_float,
+                                           ct.POINTER(ct.c_float), fp]),
+        "amrlbm_net_train_step": (ct.c_int, [vp, ct.c_int32, fp, fp, ct.c_float, ct.c_float,
+                                             ct.POINTER(ct.c_float)]),
+        "amrlbm_net_selftest_gemm": (ct.c_int, [ct.c_int32, ct.c_int32, ct.c_int32,
+                                                ct.POINTER(ct.c_uint16), ct.POINTER(ct.c_uint16),
+                                                fp]),
         "amrlbm_create_batch": (ct.c_int, [ct.POINTER(Params), ct.c_int32, ct.POINTER(Instance),
                                            ct.POINTER(vp)]),
         "amrlbm_get_instances": (ct.c_int, [vp, i32p]),
@@ -704,3 +719,81 @@ def autotune(instances, precision="fp16", block_sizes=(16, 8), ctas=(0, 1, 2, 3,
             sim.close()
     best = max(table, key=lambda r: r["mlups"]) if table else None
     return best, table
+
+
+# ---------------------------------------------------------------------------
+# The refine-flag forecaster of the learned regrid (amrlbm_net_*).
+NET_CHANNELS, NET_TILE = 4, 18
+
+
+class Net:
+    """The convolutional refine-flag forecaster: forward, gradient, Adam
+    steps on BF16 tensor cores (amrlbm_net_*). Samples are float32 arrays
+    [n][NET_CHANNELS][NET_TILE][NET_TILE], labels float32 in {0, 1}."""
+
+    def __init__(self, seed: int = 0, max_batch: int = 512, lib=None):
+        self.lib = lib or load_library()
+        self.max_batch = max_batch
+        h = ct.c_void_p()
+        st = self.lib.amrlbm_net_create(seed, max_batch, ct.byref(h))
+        if st != 0:
+            raise AmrLbmError(st, "amrlbm_net_create failed (is a B200 visible?)")
+        self.h = h
+        self.nparam = int(self.lib.amrlbm_net_param_count())
+
+    def _check(self, st):
+        if st != 0:
+            raise AmrLbmError(st, self.lib.amrlbm_net_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.amrlbm_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _f(a):
+        return np.ascontiguousarray(a, dtype=np.float32)
+
+    def params(self):
+        p = np.zeros(self.nparam, dtype=np.float32)
+        self._check(self.lib.amrlbm_net_get(self.h, _ptr(p, ct.c_float)))
+        return p
+
+    def set_params(self, p):
+        p = self._f(p)
+        assert p.size == self.nparam
+        self._check(self.lib.amrlbm_net_set(self.h, _ptr(p, ct.c_float)))
+
+    def forward(self, x):
+        x = self._f(x)
+        out = np.zeros(len(x), dtype=np.float32)
+        for i in range(0, len(x), self.max_batch):
+            xb = np.ascontiguousarray(x[i:i + self.max_batch])
+            ob = np.zeros(len(xb), dtype=np.float32)
+            self._check(self.lib.amrlbm_net_forward(self.h, len(xb), _ptr(xb, ct.c_float),
+                                                    _ptr(ob, ct.c_float)))
+            out[i:i + len(xb)] = ob
+        return out
+
+    def gradient(self, x, y, pos_weight=1.0):
+        x, y = self._f(x), self._f(y)
+        loss = ct.c_float()
+        g = np.zeros(self.nparam, dtype=np.float32)
+        self._check(self.lib.amrlbm_net_gradient(self.h, len(x), _ptr(x, ct.c_float),
+                                                 _ptr(y, ct.c_float), pos_weight, ct.byref(loss),
+                                                 _ptr(g, ct.c_float)))
+        return loss.value, g
+
+    def train_step(self, x, y, lr=1e-3, pos_weight=1.0):
+        x, y = self._f(x), self._f(y)
+        loss = ct.c_float()
+        self._check(self.lib.amrlbm_net_train_step(self.h, len(x), _ptr(x, ct.c_float),
+                                                   _ptr(y, ct.c_float), pos_weight, lr,
+                                                   ct.byref(loss)))
+        return loss.value

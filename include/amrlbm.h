@@ -316,6 +316,41 @@ int amrlbm_get_instances(amrlbm_ctx* ctx, int32_t* inst);
  * each instance's sums in leaf-list order. */
 int amrlbm_diag_instances(amrlbm_ctx* ctx, double* out);
 
+/* ---- learned regrid: the refine-flag forecaster ---------------------------
+ * No counterpart in the reference, which flags blocks from the current field
+ * only (Err_Interface, Refine_Derefine.f90:327-351). A small convolutional
+ * network over one 16x16 block with its ghost ring (AMRLBM_NET_CHANNELS
+ * channels on AMRLBM_NET_TILE^2 cells, layout [n][channel][y][x]): three 3x3
+ * convolutions of 32 channels with ReLU, a global max pool, a dense output;
+ * the logit of "this block is flagged for refinement k steps from now". BF16
+ * weights and activations on the tensor cores, FP32 accumulation, FP32 master
+ * weights trained with Adam on a weighted binary cross-entropy. Parameter
+ * vector (amrlbm_net_param_count floats): W1 [36][32], b1, W2 [288][32], b2,
+ * W3 [288][32], b3, wd [32], bd, with W[(ci*9 + (dy+1)*3 + (dx+1))][co]. */
+#define AMRLBM_NET_CHANNELS 4
+#define AMRLBM_NET_TILE 18
+typedef struct amrlbm_net amrlbm_net;
+int amrlbm_net_create(uint64_t seed, int32_t max_batch, amrlbm_net** out);
+int amrlbm_net_destroy(amrlbm_net* net);
+int32_t amrlbm_net_param_count(void);
+const char* amrlbm_net_last_error(const amrlbm_net* net);
+int amrlbm_net_get(amrlbm_net* net, float* params);
+/* also resets the optimiser state */
+int amrlbm_net_set(amrlbm_net* net, const float* params);
+/* logits of n samples x (host memory) */
+int amrlbm_net_forward(amrlbm_net* net, int32_t n, const float* x, float* logits);
+/* mean loss and its gradient (host, param_count floats; may be NULL) over n
+ * samples with labels y in {0, 1}, positives weighted pos_weight */
+int amrlbm_net_gradient(amrlbm_net* net, int32_t n, const float* x, const float* y,
+                        float pos_weight, float* loss, float* grad);
+/* one Adam step (learning rate lr) on the gradient of n samples */
+int amrlbm_net_train_step(amrlbm_net* net, int32_t n, const float* x, const float* y,
+                          float pos_weight, float lr, float* loss);
+/* the network's tensor-core product alone: C = A B, A [M][K] and B [K][N]
+ * BF16 bit patterns, C FP32, row-major host arrays */
+int amrlbm_net_selftest_gemm(int32_t M, int32_t N, int32_t K, const uint16_t* A,
+                             const uint16_t* B, float* C);
+
 /* ---- download without allocation ----------------------------------------
  * No counterpart in the reference, whose fields live in host memory.
  * amrlbm_download_fields with the same arguments and results, for callers
