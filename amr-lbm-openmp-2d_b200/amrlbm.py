@@ -278,6 +278,10 @@ def load_library(path: str | None = None):
         "amrlbm_set_precision": (ct.c_int, [vp, ct.c_int32]),
         "amrlbm_get_fill_order": (ct.c_int, [vp, i32p]),
         "amrlbm_set_launch": (ct.c_int, [vp, ct.c_int32]),
+        "amrlbm_set_bubbles": (ct.c_int, [vp, ct.c_int32, dp]),
+        "amrlbm_block_features": (ct.c_int, [vp, ct.c_int32, i32p, ct.c_float, fp]),
+        "amrlbm_set_regrid_net": (ct.c_int, [vp, vp, ct.c_float, ct.c_float]),
+        "amrlbm_regrid_stats": (ct.c_int, [vp, ct.POINTER(ct.c_int64)]),
         "amrlbm_net_create": (ct.c_int, [ct.c_uint64, ct.c_int32, ct.POINTER(vp)]),
         "amrlbm_net_destroy": (ct.c_int, [vp]),
         "amrlbm_net_param_count": (ct.c_int32, []),
@@ -440,6 +444,32 @@ class AmrLbm:
         if isinstance(precision, str):
             precision = {"fp64": FP64, "fp16": FP16, "bf16": BF16}[precision.lower()]
         self._check(self.lib.amrlbm_set_precision(self.ctx, int(precision)))
+
+    def set_bubbles(self, xyr):
+        """Several bubbles (rows x, y, R) for the start-up (amrlbm_set_bubbles)."""
+        a = np.ascontiguousarray(np.asarray(xyr, dtype=np.float64).reshape(-1, 3))
+        self._check(self.lib.amrlbm_set_bubbles(self.ctx, len(a), _ptr(a, ct.c_double)))
+
+    def block_features(self, ids, horizon: float = 16.0):
+        """The forecaster's samples of blocks ids (amrlbm_block_features):
+        float32 [n][4][18][18]."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        x = np.zeros((len(ids), NET_CHANNELS, NET_TILE, NET_TILE), dtype=np.float32)
+        self._check(self.lib.amrlbm_block_features(self.ctx, len(ids), _ptr(ids, ct.c_int32),
+                                                   horizon, _ptr(x, ct.c_float)))
+        return x
+
+    def set_regrid_net(self, net, horizon: float = 16.0, threshold: float = 0.5):
+        """Learned regrid with the forecaster `net` (a Net; None: the
+        criterion alone), amrlbm_set_regrid_net."""
+        self._net = net
+        self._check(self.lib.amrlbm_set_regrid_net(self.ctx, net.h if net else None, horizon,
+                                                   threshold))
+
+    def regrid_stats(self):
+        a = (ct.c_int64 * 5)()
+        self._check(self.lib.amrlbm_regrid_stats(self.ctx, a))
+        return dict(zip(("regrids", "forecast", "flagged", "missed", "extra"), list(a)))
 
     def set_launch(self, ctas_per_sm: int = 0):
         """At most ctas_per_sm CTAs per SM for the mixed-precision kernels
@@ -797,3 +827,107 @@ class Net:
                                                    _ptr(y, ct.c_float), pos_weight, lr,
                                                    ct.byref(loss)))
         return loss.value
+
+
+# ---------------------------------------------------------------------------
+# The learned-regrid workload: several bubbles in one domain.
+
+def random_bubbles(count: int, rmin: float, rmax: float, width: float, height: float,
+                   seed: int, margin: float = 8.0, ymax_frac: float = 0.5):
+    """count non-overlapping bubbles (rows x, y, R), R uniform in [rmin, rmax],
+    centres uniform in the domain's lower ymax_frac, `margin` cells apart
+    and from the walls (periodic in x)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    tries = 0
+    while len(out) < count:
+        tries += 1
+        if tries > 100000:
+            raise ValueError("bubbles do not fit")
+        R = float(rng.uniform(rmin, rmax))
+        x = float(rng.uniform(0.0, width))
+        y = float(rng.uniform(R + margin, ymax_frac * height - R - margin))
+        ok = True
+        for (x2, y2, R2) in out:
+            dxp = min(abs(x - x2), width - abs(x - x2))
+            if (dxp ** 2 + (y - y2) ** 2) ** 0.5 < R + R2 + margin:
+                ok = False
+                break
+        if ok:
+            out.append((x, y, R))
+    return np.array(out)
+
+
+def learned_workload(base_x: int = 512, base_y: int = 1024, levels: int = 3, count: int = 8,
+                     seed: int = 20261205, rmin: float = 32.0, rmax: float = 128.0,
+                     regrid_every: int = 32, rho_ratio: float = 1000.0,
+                     visc_ratio: float = 100.0, eo: float = 20.0, ar: float = 40.0,
+                     gy: float | None = None, refin_tol: float = 1e-3,
+                     deref_tol: float = 5e-4):
+    """Learned regrid: base grid base_x x base_y in 16x16 blocks with `levels`
+    refinement levels, `count` non-overlapping bubbles R in [rmin, rmax]; by
+    default density ratio 1000, viscosity ratio 100, Eo 20, Ar 40 (the
+    reference's), Gy such that Gy D^3 / Ar^2 with D = 128 equals the reference
+    start-up bubble's (as LARGE_GY does), hydrostatic start. Returns
+    (params, bubbles)."""
+    W, H = base_x * 2 ** levels, base_y * 2 ** levels
+    bubbles = random_bubbles(count, rmin, rmax, W, H, seed)
+    if gy is None:
+        gy = 5e-6 * 51.2 ** 3 / 40.0 ** 2 * ar ** 2 / 128.0 ** 3
+    p = bubble_params(base_x, base_y, levels, float(bubbles[0, 2]), float(bubbles[0, 0]),
+                      float(bubbles[0, 1]), rho_ratio, visc_ratio, eo, eo ** 3 / ar ** 4,
+                      regrid_every=regrid_every, gy=gy, refin_tol=refin_tol, deref_tol=deref_tol)
+    p.ar = ar
+    return p, bubbles
+
+
+def collect_samples(sim: "AmrLbm", regrids: int, horizon: int = 16, keep_far: float = 0.1,
+                    seed: int = 0):
+    """Samples of the forecaster from a run of `sim` whose regrid interval is
+    2*horizon: at each regrid (step t), the samples of the leaves that may
+    still refine, labelled with the reference's criterion at step t + horizon
+    (no regrid in between, so the blocks are the same). Leaves with nothing
+    near an interface (every cell's error term below a tenth of the tolerance
+    and no flag) are kept with probability keep_far. Returns (x, y, counts)."""
+    rng = np.random.default_rng(seed)
+    R = sim.params.regrid_every
+    assert R == 2 * horizon
+    xs, ys = [], []
+    seen = pos = 0
+    for _ in range(regrids):
+        t = sim.topology()
+        leaves = sim.leaves()
+        lv = t["level"][leaves - 1]
+        cand = leaves[lv < sim.params.max_levels]
+        x = sim.block_features(cand, float(horizon))
+        sim.main_loop(horizon)
+        err = sim.block_errors()
+        y = (err[cand - 1] > sim.params.refin_tol).astype(np.float32)
+        sim.main_loop(R - horizon)
+        near = (x[:, 1].reshape(len(x), -1).max(axis=1) > np.log1p(0.1)) | (y > 0)
+        keep = near | (rng.random(len(x)) < keep_far)
+        seen += len(x)
+        pos += int(y.sum())
+        xs.append(x[keep].astype(np.float16))
+        ys.append(y[keep])
+    return (np.concatenate(xs), np.concatenate(ys),
+            {"samples": seen, "positives": pos, "kept": int(sum(len(a) for a in ys))})
+
+
+def train_net(net: "Net", x, y, epochs: int = 4, batch: int = 512, lr: float = 2e-3,
+              seed: int = 0):
+    """Adam on the samples, positives weighted by the class ratio; returns
+    the mean loss of each epoch."""
+    rng = np.random.default_rng(seed)
+    npos = max(float(y.sum()), 1.0)
+    pw = float(min(max((len(y) - npos) / npos, 1.0), 50.0))
+    losses = []
+    for _ in range(epochs):
+        order = rng.permutation(len(y))
+        tot, cnt = 0.0, 0
+        for i in range(0, len(order) - batch + 1, batch):
+            idx = order[i:i + batch]
+            tot += net.train_step(x[idx].astype(np.float32), y[idx], lr=lr, pos_weight=pw)
+            cnt += 1
+        losses.append(tot / max(cnt, 1))
+    return losses

@@ -59,6 +59,14 @@ struct amrlbm_ctx {
     bool fp64_stale = false;  // the mixed-precision state is newer than the FP64 pool
     std::vector<amrlbm_instance> insts;  // batched instances (amrlbm_create_batch)
     unsigned char* d_active = nullptr;   // s.inst_active
+    std::vector<double> bubbles;         // several bubbles (x, y, R) (amrlbm_set_bubbles)
+    // learned regrid (amrlbm_set_regrid_net)
+    amrlbm_net* net = nullptr;
+    float net_horizon = 16.f, net_logit = 0.f;
+    int64_t rstats[5] = {0, 0, 0, 0, 0};
+    float* d_feat = nullptr;
+    int* d_fids = nullptr;
+    size_t feat_cap = 0;
 };
 
 namespace {
@@ -590,6 +598,8 @@ int amrlbm_destroy(amrlbm_ctx* ctx) {
     if (ctx->d_stage) cudaFree(ctx->d_stage);
     if (ctx->d_ids) cudaFree(ctx->d_ids);
     if (ctx->d_flush) cudaFree(ctx->d_flush);
+    if (ctx->d_feat) cudaFree(ctx->d_feat);
+    if (ctx->d_fids) cudaFree(ctx->d_fids);
     if (ctx->t0) cudaEventDestroy(ctx->t0);
     if (ctx->t1) cudaEventDestroy(ctx->t1);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -955,9 +965,41 @@ int amrlbm_init_fields(amrlbm_ctx* ctx) {
         CK(cudaMemcpy(inst.data(), ctx->s.inst, inst.size() * sizeof(int), cudaMemcpyDeviceToHost));
     }
     std::vector<double> C(leaves.size() * cs);
+    const size_t ps = (size_t)nx * ny;
+    const int nb = (int)ctx->bubbles.size() / 3;  // several bubbles: C and P from the nearest
+    std::vector<double> P(nb ? leaves.size() * ps : 0);
     for (size_t m = 0; m < leaves.size(); ++m) {
         const int n = leaves[m];
         const int dx = t.dx[n];
+        if (nb) {
+            const double W = ctx->s.ph.W;
+            const PhysD& ph = ctx->s.ph;
+            for (int j = -1; j <= ny + 2; ++j)
+                for (int i = -1; i <= nx + 2; ++i) {
+                    const double Xc = (double)(t.bi[n] * dx * nx) + dx * (i - 0.5);
+                    const double Yc = (double)(t.bj[n] * dx * ny) + dx * (j - 0.5);
+                    double dmin = 1e300;
+                    int kb = 0;
+                    for (int k = 0; k < nb; ++k) {
+                        const double* b = &ctx->bubbles[3 * k];
+                        const double d = std::sqrt((Xc - b[0]) * (Xc - b[0]) + (Yc - b[1]) * (Yc - b[1])) - b[2];
+                        if (d < dmin) {
+                            dmin = d;
+                            kb = k;
+                        }
+                    }
+                    const double c = 0.5 + 0.5 * std::tanh(2.0 * dmin / W);
+                    C[m * cs + (i + 1) + (nx + 4) * (j + 1)] = c;
+                    if (i >= 1 && i <= nx && j >= 1 && j <= ny) {
+                        const double* b = &ctx->bubbles[3 * kb];
+                        double pv = -ph.Sigma / b[2] * c;
+                        if (ctx->prm.hydrostatic_start)
+                            pv = pv + ph.Gy * (ph.Rhoh - ph.Rhol) * (1.0 - c) * (Yc - b[1]);
+                        P[m * ps + (i - 1) + nx * (j - 1)] = pv;
+                    }
+                }
+            continue;
+        }
         const amrlbm_instance* bi = ctx->s.n_inst ? &ctx->insts[inst[n]] : nullptr;
         const double R = bi ? bi->radius : ctx->prm.radius, X0 = bi ? bi->xc : ctx->prm.xc,
                      Y0 = bi ? bi->yc : ctx->prm.yc, W = bi ? bi->w : ctx->s.ph.W;
@@ -972,11 +1014,11 @@ int amrlbm_init_fields(amrlbm_ctx* ctx) {
     }
     if (!leaves.empty()) {
         if (int r = upload_blocks(ctx, (int)leaves.size(), leaves.data(), nullptr, nullptr,
-                                  C.data(), nullptr, nullptr, nullptr))
+                                  C.data(), nb ? P.data() : nullptr, nullptr, nullptr))
             return r;
     }
     launch_init_fields(ctx->s, ctx->lc, ctx->st, ctx->prm.radius, ctx->prm.hydrostatic_start,
-                       ctx->prm.yc);
+                       ctx->prm.yc, nb ? 1 : 0);
     ctx->tail_done = true;
     return sync_check(ctx);
 }
@@ -1106,6 +1148,8 @@ int amrlbm_regrid(amrlbm_ctx* ctx, double refin_tol, double deref_tol) {
     return sync_check(ctx);
 }
 
+int learned_regrid(amrlbm_ctx* ctx);
+
 int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
     if (!ctx || nsteps < 0) return AMRLBM_ERR_ARG;
     if (nsteps == 0) return AMRLBM_OK;
@@ -1124,6 +1168,7 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
         const bool final_chunk = (done + chunk == nsteps);
         const auto key = std::make_tuple(chunk, phase, ctx->tail_done ? 1 : 0, final_chunk ? 1 : 0,
                                          ctx->prof ? 1 : 0);
+        const bool learned = ctx->net != nullptr;  // the regrid runs after the graph
         if (ctx->prof_pending) {  // the previous replay's events must be read first
             CK(cudaStreamSynchronize(ctx->st));
             harvest_profile(ctx);
@@ -1137,7 +1182,8 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
             for (int t = 0; t < chunk; ++t) {
                 const bool regrid = ((phase + t + 1) % R) == 0;
                 const bool tail = regrid || (final_chunk && t == chunk - 1);
-                enqueue_step(ctx, &ge, prev_tail, tail, regrid, final_chunk && t == chunk - 1);
+                enqueue_step(ctx, &ge, prev_tail, tail, regrid && !learned,
+                             (final_chunk && t == chunk - 1) || (regrid && learned));
                 prev_tail = tail;
             }
             cudaGraph_t g;
@@ -1160,6 +1206,9 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
         ctx->stepcount += chunk;
         ctx->tail_done = last_tail;
         done += chunk;
+        if (learned && ctx->stepcount % R == 0) {
+            if (int r = learned_regrid(ctx)) return r;
+        }
     }
     CK(cudaGetLastError());
     return AMRLBM_OK;
@@ -1700,6 +1749,132 @@ int amrlbm_diag_instances(amrlbm_ctx* ctx, double* out) {
         if (a[8] != 0.0) bad = true;
     }
     if (bad) return fail(ctx, AMRLBM_ERR_NAN, "non-finite C or Uy in a leaf");
+    return AMRLBM_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Several bubbles and the learned regrid. No counterpart in the reference
+// (one bubble; Refine_Derefine_Mesh from the current field only).
+extern "C" int amrlbm_net_forward_device(amrlbm_net* net, int32_t n, const float* x_dev,
+                                         float* logits);
+
+namespace {
+
+// the forecaster's samples of blocks ids[0..n) into ctx->d_feat
+int features_to_device(amrlbm_ctx* ctx, int n, const int* ids, float horizon) {
+    const size_t per = (size_t)AMRLBM_NET_CHANNELS * (ctx->prm.nx + 2) * (ctx->prm.ny + 2);
+    if ((size_t)n > ctx->feat_cap) {
+        if (ctx->d_feat) cudaFree(ctx->d_feat);
+        if (ctx->d_fids) cudaFree(ctx->d_fids);
+        ctx->d_feat = nullptr;
+        ctx->d_fids = nullptr;
+        const size_t cap = (size_t)n + n / 2 + 64;
+        CK(cudaMalloc(&ctx->d_feat, cap * per * sizeof(float)));
+        CK(cudaMalloc(&ctx->d_fids, cap * sizeof(int)));
+        ctx->feat_cap = cap;
+    }
+    if (n == 0) return AMRLBM_OK;
+    CK(cudaMemcpyAsync(ctx->d_fids, ids, n * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    launch_block_features(ctx->s, ctx->st, n, ctx->d_fids, horizon, ctx->prm.refin_tol, ctx->d_feat);
+    return AMRLBM_OK;
+}
+
+}  // namespace
+
+// Refine_Derefine_Mesh with the forecaster: every leaf that may still refine
+// is refined if the forecaster expects it flagged within its horizon or if
+// the reference's criterion (Err_Interface > refin_tol, Refine_Derefine.f90:
+// 36-40) flags it now; a leaf the criterion flags and the forecaster missed
+// is counted. The forecast enters the regrid as the leaf's error raised to
+// twice the tolerance, which also keeps its parent from derefining.
+int learned_regrid(amrlbm_ctx* ctx) {
+    CK(cudaStreamSynchronize(ctx->st));
+    ensure_fp64(ctx, true);
+    const Counters c = read_counters(ctx);
+    std::vector<int> leaves;
+    HostTopo t;
+    if (int r = get_leaves_host(ctx, leaves, t)) return r;
+    std::vector<int> inst;
+    if (ctx->s.n_inst) {
+        inst.resize(t.dx.size());
+        CK(cudaMemcpy(inst.data(), ctx->s.inst, inst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    std::vector<double> err((size_t)c.nblks + 1);
+    CK(cudaMemcpy(err.data(), ctx->s.err, err.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<int> cand;
+    for (int n : leaves) {
+        const int mlv = ctx->s.n_inst ? ctx->insts[inst[n]].max_levels : ctx->prm.max_levels;
+        if (t.level[n] < mlv && t.level[n] >= c.level_min && t.level[n] <= c.level_max) cand.push_back(n);
+    }
+    std::vector<float> logit(cand.size());
+    if (int r = features_to_device(ctx, (int)cand.size(), cand.data(), ctx->net_horizon)) return r;
+    if (!cand.empty()) {
+        CK(cudaStreamSynchronize(ctx->st));
+        if (int r = amrlbm_net_forward_device(ctx->net, (int)cand.size(), ctx->d_feat, logit.data()))
+            return fail(ctx, r, "forecaster forward");
+    }
+    const double rt = ctx->prm.refin_tol;
+    int64_t pred = 0, crit = 0, missed = 0, extra = 0;
+    for (size_t i = 0; i < cand.size(); ++i) {
+        const int n = cand[i];
+        const bool p = logit[i] > ctx->net_logit, k = err[n] > rt;
+        pred += p;
+        crit += k;
+        missed += (k && !p);
+        extra += (p && !k);
+        if (p && !k) err[n] = 2.0 * rt;
+    }
+    CK(cudaMemcpy(ctx->s.err, err.data(), err.size() * sizeof(double), cudaMemcpyHostToDevice));
+    enqueue_regrid(ctx, rt, ctx->prm.deref_tol, false, true);
+    ctx->tail_done = true;
+    ctx->rstats[0] += 1;
+    ctx->rstats[1] += pred;
+    ctx->rstats[2] += crit;
+    ctx->rstats[3] += missed;
+    ctx->rstats[4] += extra;
+    return sync_check(ctx);
+}
+
+extern "C" {
+
+int amrlbm_set_bubbles(amrlbm_ctx* ctx, int32_t n, const double* xyr) {
+    if (!ctx || n < 0 || (n > 0 && !xyr) || ctx->s.n_inst) return AMRLBM_ERR_ARG;
+    for (int i = 0; i < n; ++i)
+        if (!(xyr[3 * i + 2] > 0.0)) return AMRLBM_ERR_ARG;
+    ctx->bubbles.assign(xyr, xyr + 3 * (size_t)n);
+    return AMRLBM_OK;
+}
+
+int amrlbm_block_features(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, float horizon, float* x) {
+    if (!ctx || n < 0 || (n > 0 && (!ids || !x))) return AMRLBM_ERR_ARG;
+    if (ctx->prm.nx + 2 != AMRLBM_NET_TILE || ctx->prm.ny + 2 != AMRLBM_NET_TILE)
+        return fail(ctx, AMRLBM_ERR_ARG, "the forecaster takes 16x16 blocks");
+    for (int i = 0; i < n; ++i)
+        if (ids[i] < 1 || ids[i] > ctx->prm.max_blks) return AMRLBM_ERR_ARG;
+    ensure_fp64(ctx, false);
+    if (int r = features_to_device(ctx, n, ids, horizon)) return r;
+    const size_t per = (size_t)AMRLBM_NET_CHANNELS * AMRLBM_NET_TILE * AMRLBM_NET_TILE;
+    if (n) CK(cudaMemcpyAsync(x, ctx->d_feat, (size_t)n * per * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    return sync_check(ctx);
+}
+
+int amrlbm_set_regrid_net(amrlbm_ctx* ctx, amrlbm_net* net, float horizon, float threshold) {
+    if (!ctx || (net && (!(horizon > 0.f) || !(threshold > 0.f) || !(threshold < 1.f))))
+        return AMRLBM_ERR_ARG;
+    if (net && (ctx->prm.nx != 16 || ctx->prm.ny != 16))
+        return fail(ctx, AMRLBM_ERR_ARG, "the forecaster takes 16x16 blocks");
+    ctx->net = net;
+    ctx->net_horizon = horizon;
+    ctx->net_logit = net ? std::log(threshold / (1.f - threshold)) : 0.f;
+    drop_graphs(ctx);
+    return AMRLBM_OK;
+}
+
+int amrlbm_regrid_stats(amrlbm_ctx* ctx, int64_t out[5]) {
+    if (!ctx || !out) return AMRLBM_ERR_ARG;
+    for (int i = 0; i < 5; ++i) out[i] = ctx->rstats[i];
     return AMRLBM_OK;
 }
 

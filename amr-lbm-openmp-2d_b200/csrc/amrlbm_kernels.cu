@@ -38,7 +38,9 @@ __device__ __forceinline__ void ring1_xy(int r, int nx, int ny, int& x, int& y) 
 // Initialize_AMR_Rising_Bubble (AMR_Rising_2D_OMP.f90:186-226) given C
 // hydro != 0: P also carries the light phase's hydrostatic head about the
 // bubble centre y0, Gy*(Rhoh-Rhol)*(1-C)*(y-y0) (amrlbm_params.hydrostatic_start)
-__global__ void __launch_bounds__(256) k_init_fields(DevState s, double R0, int hydro0, double Y00) {
+// p_given: P of every leaf was uploaded (several bubbles), not derived here
+__global__ void __launch_bounds__(256) k_init_fields(DevState s, double R0, int hydro0, double Y00,
+                                                     int p_given) {
     extern __shared__ double T[];
     const int nleaf = s.cnt->nleaf, nx = s.nx, ny = s.ny, TW = nx + 4;
     for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
@@ -56,8 +58,8 @@ __global__ void __launch_bounds__(256) k_init_fields(DevState s, double R0, int 
             auto Cs = [&](int ddx, int ddy) { return T[(y + ddy + 1) * TW + (x + ddx + 1)]; };
             const double Cij = Cs(0, 0);
             const double Ux = 0, Uy = 0;
-            double P = -ph.Sigma / R * Cij;
-            if (hydro) {
+            double P = p_given ? s.P[p_idx(s, n, x, y)] : -ph.Sigma / R * Cij;
+            if (hydro && !p_given) {
                 const double Yc = (double)(s.bj[n] * dx * ny) + dx * (y - 0.5);
                 P = P + ph.Gy * (ph.Rhoh - ph.Rhol) * (1.0 - Cij) * (Yc - Y0);
             }
@@ -747,6 +749,32 @@ __global__ void k_diag_final(DevState s, const double* part, double* out) {
     }
 }
 
+// Samples of the refine-flag forecaster for blocks ids[0..n): per block 4
+// channels on its (nx+2)^2 cells, ring 1 included ([i][channel][y][x]): C;
+// log(1 + e/tol) with e the cell's Err_Interface term sqrt(dCx^2 + dCy^2)/(2dx)
+// (Refine_Derefine.f90:327-351), so the refine criterion is e > tol; Ux and Uy
+// times horizon/dx, the cells the flow moves over the horizon (0 on the ring).
+// Needs C's ghost rings of the current state (between amrlbm_step calls).
+__global__ void k_block_features(DevState s, int n, const int* ids, float horizon, double tol,
+                                 float* out) {
+    const int nx = s.nx, ny = s.ny, W = nx + 2, P = W * (ny + 2);
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int b = ids[i];
+        const double dx = (double)s.dx[b];
+        float* o = out + (size_t)i * 4 * P;
+        for (int c = threadIdx.x; c < P; c += blockDim.x) {
+            const int x = c % W, y = c / W;
+            const double gx = s.C[c_idx(s, b, x + 1, y)] - s.C[c_idx(s, b, x - 1, y)];
+            const double gy = s.C[c_idx(s, b, x, y + 1)] - s.C[c_idx(s, b, x, y - 1)];
+            o[c] = (float)s.C[c_idx(s, b, x, y)];
+            o[P + c] = (float)log1p(sqrt(gx * gx + gy * gy) / (2.0 * dx) / tol);
+            const bool in = x >= 1 && x <= nx && y >= 1 && y <= ny;
+            o[2 * P + c] = in ? (float)(s.Ux[p_idx(s, b, x, y)] * horizon / dx) : 0.f;
+            o[3 * P + c] = in ? (float)(s.Uy[p_idx(s, b, x, y)] * horizon / dx) : 0.f;
+        }
+    }
+}
+
 size_t tile_bytes(const DevState& s) { return (size_t)(s.nx + 4) * (s.ny + 4) * sizeof(double); }
 int block_threads(const DevState& s) {
     const int t = ((s.nx * s.ny + 31) / 32) * 32;
@@ -776,9 +804,15 @@ void launch_minmax(const DevState& s, cudaStream_t st) {
     count_launches(1);
 }
 
+void launch_block_features(const DevState& s, cudaStream_t st, int n, const int* ids,
+                           float horizon, double tol, float* out) {
+    k_block_features<<<n < 4096 ? (n > 0 ? n : 1) : 4096, 128, 0, st>>>(s, n, ids, horizon, tol, out);
+    count_launches(1);
+}
+
 void launch_init_fields(const DevState& s, const LaunchCfg& lc, cudaStream_t st, double radius,
-                        int hydro, double y0) {
-    k_init_fields<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s, radius, hydro, y0);
+                        int hydro, double y0, int p_given) {
+    k_init_fields<<<lc.grid_leaves, block_threads(s), tile_bytes(s), st>>>(s, radius, hydro, y0, p_given);
     count_launches(1);
 }
 

@@ -34,7 +34,9 @@ void launch_macro_g(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_err(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 void launch_minmax(const DevState& s, cudaStream_t st);
 void launch_init_fields(const DevState& s, const LaunchCfg& lc, cudaStream_t st, double radius,
-                        int hydro, double y0);
+                        int hydro, double y0, int p_given = 0);
+void launch_block_features(const DevState& s, cudaStream_t st, int n, const int* ids,
+                           float horizon, double tol, float* out);
 void launch_regrid_flags(const DevState& s, cudaStream_t st, double refin_tol, double deref_tol);
 void launch_restrict(const DevState& s, const LaunchCfg& lc, cudaStream_t st);
 // mode 0: Refine_Derefine_Mesh; 1: Initial_Mesh level (no data movement);

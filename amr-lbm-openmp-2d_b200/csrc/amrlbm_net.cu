@@ -16,6 +16,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -485,6 +486,25 @@ int amrlbm_net_forward(amrlbm_net* net, int32_t n, const float* x, float* logits
                                                net->logits, net->dlogit, net->lterm);
     count_launches(1);
     NCK(cudaMemcpyAsync(logits, net->logits, sizeof(float) * n, cudaMemcpyDeviceToHost, net->st));
+    NCK(cudaStreamSynchronize(net->st));
+    return AMRLBM_OK;
+}
+
+// forward of samples already in device memory (the learned regrid's
+// features), logits to the host; n may exceed the batch capacity
+int amrlbm_net_forward_device(amrlbm_net* net, int32_t n, const float* x_dev, float* logits) {
+    if (!net || !logits || n < 0 || (n > 0 && !x_dev)) return AMRLBM_ERR_ARG;
+    const size_t per = (size_t)CIN * PIX;
+    for (int i0 = 0; i0 < n; i0 += net->max_n) {
+        const int b = std::min(net->max_n, n - i0);
+        NCK(cudaMemcpyAsync(net->x, x_dev + per * i0, sizeof(float) * per * b,
+                            cudaMemcpyDeviceToDevice, net->st));
+        forward(net, b);
+        k_head<<<blocks_for(b), 256, 0, net->st>>>(b, net->pooled, net->p + O_WD, nullptr, 1.f,
+                                                   net->logits, net->dlogit, net->lterm);
+        count_launches(1);
+        NCK(cudaMemcpyAsync(logits + i0, net->logits, sizeof(float) * b, cudaMemcpyDeviceToHost, net->st));
+    }
     NCK(cudaStreamSynchronize(net->st));
     return AMRLBM_OK;
 }

@@ -34,7 +34,10 @@ Beside the FP64 value: mixed_precision (the same workload with FP16 / BF16
 population storage, MLUPS), mixed_precision_error (the 64x128-base bubble in
 FP16 and BF16 against FP64 at steps 1000 / 2500 / 5000: rise velocity,
 centroid, mass), batched (the seeded batch of 256 uneven problems in one pool,
-block size and CTAs per SM chosen by amrlbm.autotune, FP64 and FP16 MLUPS).
+block size and CTAs per SM chosen by amrlbm.autotune, FP64 and FP16 MLUPS),
+learned_regrid (the 8-bubble learned-regrid configuration: forecaster samples
+seen and trained on, then the criterion every 10 steps against the learned
+regrid every 32: regrids, escapes, misses, MLUPS).
 """
 from __future__ import annotations
 
@@ -375,6 +378,67 @@ def batched_leg(count=256, tune_count=32, intervals=3):
     return res
 
 
+def learned_leg(samples_target=1_000_000, eval_steps=960):
+    """Learned regrid on its configuration (512x1024 base, 3 levels, 8
+    bubbles R in [32, 128], density ratio 1000, Eo 20, Ar 40; interval 32,
+    horizon 16): forecaster samples from a seeded run until samples_target
+    leaves have been seen, training, then the same start (another seed) run
+    eval_steps steps with the criterion every 10 steps and with the learned
+    regrid every 32; regrids, escapes (leaves the criterion flags at a
+    regrid), misses and MLUPS of each."""
+    import numpy as np
+    import amrlbm
+    p, bubbles = amrlbm.learned_workload(regrid_every=32)
+    g = amrlbm.AmrLbm(p)
+    g.set_bubbles(bubbles)
+    g.initialize_rising_bubble()
+    xs, ys, seen, pos, regrids = [], [], 0, 0, 0
+    while seen < samples_target and regrids < 400:
+        x, y, c = amrlbm.collect_samples(g, regrids=10, horizon=16, keep_far=0.02, seed=regrids)
+        xs.append(x)
+        ys.append(y)
+        seen, pos, regrids = seen + c["samples"], pos + c["positives"], regrids + 10
+    check_state(g.output(), "learned-regrid sample run")
+    leaves0 = g.counts()["nleaf"]
+    g.close()
+    x, y = np.concatenate(xs), np.concatenate(ys)
+    net = amrlbm.Net(seed=7, max_batch=512)
+    losses = amrlbm.train_net(net, x, y, epochs=3, batch=256)
+    out = {"workload": "learned_regrid_base512x1024_blocks16_L3_8bubbles_ratio1000",
+           "samples_seen": int(seen), "positives": int(pos), "samples_trained": int(len(y)),
+           "sample_regrids": regrids, "leaves": int(leaves0), "losses": losses}
+    p2, b2 = amrlbm.learned_workload(regrid_every=32, seed=20261206)
+    for name, every, use in (("criterion_every_10", 10, False), ("learned_every_32", 32, True)):
+        p2.regrid_every = every
+        s = amrlbm.AmrLbm(p2)
+        s.set_bubbles(b2)
+        s.initialize_rising_bubble()
+        never = None
+        if use:
+            s.set_regrid_net(net, horizon=16.0, threshold=0.5)
+        else:  # counted through a forecaster that never fires
+            never = amrlbm.Net(seed=7, max_batch=512)
+            q = never.params()
+            q[-1] = -1e4
+            never.set_params(q)
+            s.set_regrid_net(never, horizon=16.0, threshold=0.5)
+        c0 = s.profile_read(0)[2]
+        s.sync()
+        s.timer_start()
+        s.main_loop(eval_steps)
+        ms = s.timer_stop()
+        st = s.regrid_stats()
+        st["mlups"] = (s.profile_read(0)[2] - c0) / (ms / 1e3) / 1e6
+        st["leaves"] = s.counts()["nleaf"]
+        check_state(s.output(), name)
+        out[name] = st
+        s.close()
+        if never:
+            never.close()
+    net.close()
+    return out
+
+
 def run_own(args):
     world, rank, local = dist_setup("nccl")
     import amrlbm
@@ -547,10 +611,11 @@ def run_own(args):
                 "sample": f"the next {chunks4} x {inner} time steps ({el4:.1f} s) at 4 threads, "
                           f"the reference's OMP_NUM_THREADS"}
         orc.close()
-    mixed_err = batched = None
+    mixed_err = batched = learned = None
     if not args.no_mixed:
         mixed_err = mixed_error_report()
         batched = batched_leg()
+        learned = learned_leg()
     line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -560,7 +625,7 @@ def run_own(args):
             "e2e": e2e, "clocks": clk,
             "gpu_launches": int(launches), "kernels": kernels,
             "mixed_precision": mixed or None, "mixed_precision_error": mixed_err,
-            "batched": batched,
+            "batched": batched, "learned_regrid": learned,
             "leaf_cells_per_step": updates / (args.steps * inner),
             "diagnostics": {k: diag[k] for k in ("mass", "y_centroid", "rise_velocity")}}
     print(json.dumps(line), flush=True)

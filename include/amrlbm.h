@@ -346,10 +346,37 @@ int amrlbm_net_gradient(amrlbm_net* net, int32_t n, const float* x, const float*
 /* one Adam step (learning rate lr) on the gradient of n samples */
 int amrlbm_net_train_step(amrlbm_net* net, int32_t n, const float* x, const float* y,
                           float pos_weight, float lr, float* loss);
+/* logits of n samples already in device memory (any n) */
+int amrlbm_net_forward_device(amrlbm_net* net, int32_t n, const float* x_dev, float* logits);
 /* the network's tensor-core product alone: C = A B, A [M][K] and B [K][N]
  * BF16 bit patterns, C FP32, row-major host arrays */
 int amrlbm_net_selftest_gemm(int32_t M, int32_t N, int32_t K, const uint16_t* A,
                              const uint16_t* B, float* C);
+
+/* The forecaster's samples of blocks ids[0..n) of the current state (16x16
+ * blocks; between amrlbm_step calls, when C's ghost rings are filled), layout
+ * [n][4][18][18] over the block's cells with ring 1: C; log(1 + e/refin_tol)
+ * with e the cell's Err_Interface term sqrt(dCx^2 + dCy^2)/(2dx)
+ * (Refine_Derefine.f90:327-351); Ux and Uy times horizon/dx (cells moved in
+ * `horizon` steps; 0 on the ring). */
+int amrlbm_block_features(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, float horizon,
+                          float* x);
+/* Learned regrid: with net != NULL, every regrid of amrlbm_step refines the
+ * leaves the forecaster flags (probability > threshold; its samples taken
+ * with `horizon`) together with those the reference's criterion
+ * (Err_Interface > refin_tol) flags; NULL restores the criterion alone. The
+ * net must outlive its use. stats (accumulated over the context's life):
+ * [0] regrids, [1] leaves forecast, [2] leaves the criterion flagged,
+ * [3] flagged leaves the forecast missed (refined all the same), [4] leaves
+ * forecast but not flagged. */
+int amrlbm_set_regrid_net(amrlbm_ctx* ctx, amrlbm_net* net, float horizon, float threshold);
+int amrlbm_regrid_stats(amrlbm_ctx* ctx, int64_t out[5]);
+/* Several bubbles for amrlbm_init_rising_bubble / amrlbm_init_fields (n
+ * triples x, y, R in finest cells; n = 0: the params' one bubble): C is the
+ * tanh profile of the nearest bubble's surface, P as for one bubble with the
+ * nearest bubble's radius and centre. No counterpart in the reference's
+ * start-up (AMR_Rising_2D_OMP.f90:142-231), which places one bubble. */
+int amrlbm_set_bubbles(amrlbm_ctx* ctx, int32_t n, const double* xyr);
 
 /* ---- download without allocation ----------------------------------------
  * No counterpart in the reference, whose fields live in host memory.
