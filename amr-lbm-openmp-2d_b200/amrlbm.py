@@ -862,13 +862,17 @@ def learned_workload(base_x: int = 512, base_y: int = 1024, levels: int = 3, cou
                      seed: int = 20261205, rmin: float = 32.0, rmax: float = 128.0,
                      regrid_every: int = 32, rho_ratio: float = 1000.0,
                      visc_ratio: float = 100.0, eo: float = 20.0, ar: float = 40.0,
-                     gy: float | None = None, refin_tol: float = 1e-3,
-                     deref_tol: float = 5e-4):
+                     gy: float | None = None, refin_tol: float = 3e-4,
+                     deref_tol: float = 1.5e-4):
     """Learned regrid: base grid base_x x base_y in 16x16 blocks with `levels`
     refinement levels, `count` non-overlapping bubbles R in [rmin, rmax]; by
     default density ratio 1000, viscosity ratio 100, Eo 20, Ar 40 (the
     reference's), Gy such that Gy D^3 / Ar^2 with D = 128 equals the reference
-    start-up bubble's (as LARGE_GY does), hydrostatic start. Returns
+    start-up bubble's (as LARGE_GY does), hydrostatic start. Refinement
+    tolerance 3e-4: at 1e-3 the finest level ends about 6 cells inside a
+    bubble's interface, and the light phase blows up at a corner where a
+    coarser block inside the bubble meets three finer ones (R = 58: about
+    step 1750, with a regrid every 10 steps or every 32). Returns
     (params, bubbles)."""
     W, H = base_x * 2 ** levels, base_y * 2 ** levels
     bubbles = random_bubbles(count, rmin, rmax, W, H, seed)

@@ -524,7 +524,7 @@ __device__ void wall_c(const DevState& s, const Geo<N>& G, int n, const NbInfo& 
 // BGK: the collision of g is BGK_Collision_AMR (LBM_Subroutines.f90:337-344,
 // g*(1-s9) + geq*s9) instead of MRT_Collision_AMR, the alternative the
 // reference leaves commented out at :180
-template <bool SAFE, bool FUSED, bool SH, int N, bool BGK = false, bool BATCH = false>
+template <bool SAFE, bool FUSED, bool SHH, bool SHG, int N, bool BGK = false, bool BATCH = false>
 __device__ __forceinline__ unsigned collide_cell(const DevState& s, const Geo<N>& G, int n, int c,
                                                  double inv_dx, const double* T, const double* Hb,
                                                  const double* Gb) {
@@ -533,7 +533,8 @@ __device__ __forceinline__ unsigned collide_cell(const DevState& s, const Geo<N>
     const double inv_dx2 = inv_dx * inv_dx;
     const double* Hn = Hb + c;
     const double* Gn = Gb + c;
-    auto ldp = [&](const double* p) { return SH ? lds(p) : __ldg(p); };
+    auto ldh = [&](const double* p) { return SHH ? lds(p) : __ldg(p); };
+    auto ldp = [&](const double* p) { return SHG ? lds(p) : __ldg(p); };
     Div<SAFE> dv;
     {
         const int x = c % nx + 1, y = c / nx + 1;
@@ -607,7 +608,7 @@ __device__ __forceinline__ unsigned collide_cell(const DevState& s, const Geo<N>
             const double eN = (double)d_ex(k) * ni + (double)d_ey(k) * nj;
             const double Gm = wk * (1.0 + eU * (3.0 + 4.5 * eU) - U215);
             const double heq = c0 * (Gm + tmp * wk * eN);
-            s.Ah[G.a(n, k, x, y)] = ldp(Hn + (k - 1) * BP) * ph.omwc + heq * ph.wc;
+            s.Ah[G.a(n, k, x, y)] = ldh(Hn + (k - 1) * BP) * ph.omwc + heq * ph.wc;
             const double Ak = (Gm - wk) * ph.dRho3 + Gm * mu;
             const double Bk = ((double)d_ey(k) - Uy) * Gm * Fb;
             const double hc = Ak * (Ec(k) - ud_c) + Bk;
@@ -692,16 +693,31 @@ __device__ __forceinline__ unsigned macro_g_cell_f(const DevState& s, const Geo<
     dc = a * a + b * b;
     return dv.bad;
 }
+#ifndef AMR_SAFE_OUTLINE
+#define AMR_SAFE_OUTLINE 0
+#endif
+// the IEEE-division collision of one cell, out of line: the rare cells that
+// take it do not put a second copy of the collision body in the hot loop
+template <bool FUSED, bool SHH, bool SHG, int N, bool BGK, bool BATCH>
+__device__ __noinline__ void collide_cell_ieee(const DevState* s, const Geo<N> G, int n, int c,
+                                               double inv_dx, const double* T, const double* Hb,
+                                               const double* Gb) {
+    collide_cell<true, FUSED, SHH, SHG, N, BGK, BATCH>(*s, G, n, c, inv_dx, T, Hb, Gb);
+}
 // Collision of every cell of block n: the branch-free exact division path,
 // and the IEEE path for a cell whose flag says a quotient left its range.
-// SH: Hb and Gb point to shared memory (else to memory)
-template <int N, bool FUSED, bool SH, bool BGK = false, bool BATCH = false>
+// SHH, SHG: Hb, Gb point to shared memory (else to memory)
+template <int N, bool FUSED, bool SHH, bool SHG, bool BGK = false, bool BATCH = false>
 __device__ __forceinline__ void collide_block(const DevState& s, const Geo<N>& G, int n,
                                               const double* T, const double* Hb, const double* Gb) {
     const double inv_dx = 1.0 / (double)__ldg(s.dx + n);  // dx is a power of two: exact
     for (int c = threadIdx.x; c < G.nx * G.ny; c += blockDim.x)
-        if (collide_cell<false, FUSED, SH, N, BGK, BATCH>(s, G, n, c, inv_dx, T, Hb, Gb))
-            collide_cell<true, FUSED, SH, N, BGK, BATCH>(s, G, n, c, inv_dx, T, Hb, Gb);
+        if (collide_cell<false, FUSED, SHH, SHG, N, BGK, BATCH>(s, G, n, c, inv_dx, T, Hb, Gb)) {
+            if (AMR_SAFE_OUTLINE)
+                collide_cell_ieee<FUSED, SHH, SHG, N, BGK, BATCH>(&s, G, n, c, inv_dx, T, Hb, Gb);
+            else
+                collide_cell<true, FUSED, SHH, SHG, N, BGK, BATCH>(s, G, n, c, inv_dx, T, Hb, Gb);
+        }
 }
 
 // Macroscopic_Values_g_AMR of every cell of block n; returns this thread's
@@ -819,8 +835,14 @@ __device__ void stream_block(const DevState& s, const Geo<N>& G, int n, const do
     }
 }
 
+#ifndef AMR_K1_MINB
+#define AMR_K1_MINB 2
+#endif
+#ifndef AMR_K1_STAGE
+#define AMR_K1_STAGE 2
+#endif
 __host__ __device__ constexpr int fill_c_min_blocks(int consumer) {
-    return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) ? 2 : 3;
+    return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) ? AMR_K1_MINB : 3;
 }
 
 // Without level order: an item's C ring (block r.n; plan words pl, ring
@@ -869,10 +891,11 @@ __device__ void fast_ring_hg(const DevState& s, const Geo<N>& G, const int* pl, 
 // values, and without level order each stage's plan words and foreign
 // records (copied with the stage's tile).
 __host__ __device__ constexpr bool stage_h(int consumer) {
-    return consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED;
+    return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) && AMR_K1_STAGE >= 2;
 }
 __host__ __device__ constexpr bool stage_g(int consumer) {
-    return stage_h(consumer) || consumer == CONS_MACRO_G;
+    return ((consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) && AMR_K1_STAGE >= 1) ||
+           consumer == CONS_MACRO_G;
 }
 // doubles of one stage: C tile, h planes, g planes
 __host__ __device__ inline size_t stage_doubles(int cplane, int bplane, int consumer) {
@@ -916,12 +939,14 @@ __global__ void __launch_bounds__(256, fill_c_min_blocks(CONSUMER))
         atomicAdd(&s.cnt->updates, (unsigned long long)total * (unsigned long long)(G.nx * G.ny));
     // stage st: C tile at tiles + st*SD, then h planes (if staged), then g planes
     auto consume = [&](int n, const double* T) {
-        const double* Hs = T + G.cplane;
-        const double* Gs = Hs + (stage_h(CONSUMER) ? HP : 0);
+        const double* Hs = stage_h(CONSUMER) ? T + G.cplane : s.Bh + (size_t)n * HP;
+        const double* Gs = stage_g(CONSUMER) ? T + G.cplane + (stage_h(CONSUMER) ? HP : 0)
+                                             : s.Bg + (size_t)n * HP;
         if (CONSUMER == CONS_MACRO_G)
             err_reduce(s, n, macro_g_block<N, true, BATCH>(s, G, n, T, Gs), red);
         else if (CONSUMER != CONS_NONE)
-            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED, true, BGK, BATCH>(s, G, n, T, Hs, Gs);
+            collide_block<N, CONSUMER == CONS_COLLIDE_FUSED, stage_h(CONSUMER), stage_g(CONSUMER), BGK,
+                          BATCH>(s, G, n, T, Hs, Gs);
     };
     const unsigned tb = (unsigned)G.cplane * 8, hb = (unsigned)HP * 8;
     auto copy_tile = [&](int st, int nn, int c) {  // thread 0: item c, block nn
@@ -1223,7 +1248,7 @@ __global__ void __launch_bounds__(256, 2) k_collide(DevState s) {
     for (int m = blockIdx.x; m < nleaf; m += gridDim.x) {
         const int n = s.leaf[m];
         load_tile_c<N>(s, G, n, T);
-        collide_block<N, false, false, BGK, BATCH>(s, G, n, T, s.Bh + (size_t)n * 9 * G.bplane,
+        collide_block<N, false, false, false, BGK, BATCH>(s, G, n, T, s.Bh + (size_t)n * 9 * G.bplane,
                                                    s.Bg + (size_t)n * 9 * G.bplane);
         __syncthreads();
     }

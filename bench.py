@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision, error-report and batched legs")
+    ap.add_argument("--profile-precision", default=None, choices=["fp64", "fp16", "bf16"],
+                    help="profiling mode: the workload in this precision for --warmup + "
+                         "--steps intervals, nothing else")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--max-blks", type=int, default=0,
                     help="pool capacity (default: a fully refined tree); smaller pools "
@@ -383,9 +386,9 @@ def learned_leg(samples_target=1_000_000, eval_steps=960):
     bubbles R in [32, 128], density ratio 1000, Eo 20, Ar 40; interval 32,
     horizon 16): forecaster samples from a seeded run until samples_target
     leaves have been seen, training, then the same start (another seed) run
-    eval_steps steps with the criterion every 10 steps and with the learned
-    regrid every 32; regrids, escapes (leaves the criterion flags at a
-    regrid), misses and MLUPS of each."""
+    eval_steps steps with the criterion every 10 steps, the criterion every
+    32 and the learned regrid every 32; regrids, escapes (leaves the
+    criterion flags at a regrid), misses and MLUPS of each."""
     import numpy as np
     import amrlbm
     p, bubbles = amrlbm.learned_workload(regrid_every=32)
@@ -408,7 +411,8 @@ def learned_leg(samples_target=1_000_000, eval_steps=960):
            "samples_seen": int(seen), "positives": int(pos), "samples_trained": int(len(y)),
            "sample_regrids": regrids, "leaves": int(leaves0), "losses": losses}
     p2, b2 = amrlbm.learned_workload(regrid_every=32, seed=20261206)
-    for name, every, use in (("criterion_every_10", 10, False), ("learned_every_32", 32, True)):
+    for name, every, use in (("criterion_every_10", 10, False), ("criterion_every_32", 32, False),
+                             ("learned_every_32", 32, True)):
         p2.regrid_every = every
         s = amrlbm.AmrLbm(p2)
         s.set_bubbles(b2)
@@ -648,10 +652,32 @@ def _finish(world):
         dist.destroy_process_group()
 
 
+def run_profile(args):
+    """The workload in one storage precision, warm-up and timed intervals
+    only, for profiler captures of its kernels."""
+    import amrlbm
+    p = workload()
+    if args.max_blks:
+        p.max_blks = args.max_blks
+    g = amrlbm.AmrLbm(p)
+    g.initialize_rising_bubble()
+    g.set_precision(args.profile_precision)
+    for _ in range(args.warmup):
+        g.main_loop(p.regrid_every)
+    g.sync()
+    v = amrlbm.time_intervals(g, args.steps, p.regrid_every)
+    check_state(g.output(), "profile run")
+    print(json.dumps({"profile_precision": args.profile_precision, "mlups": v}), flush=True)
+    g.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_precision:
+        return run_profile(args)
     return run_own(args)
 
 
