@@ -282,6 +282,7 @@ def load_library(path: str | None = None):
         "amrlbm_block_features": (ct.c_int, [vp, ct.c_int32, i32p, ct.c_float, fp]),
         "amrlbm_set_regrid_net": (ct.c_int, [vp, vp, ct.c_float, ct.c_float]),
         "amrlbm_regrid_stats": (ct.c_int, [vp, ct.POINTER(ct.c_int64)]),
+        "amrlbm_forecast_blocks": (ct.c_int, [vp, ct.c_int32, i32p, fp]),
         "amrlbm_net_create": (ct.c_int, [ct.c_uint64, ct.c_int32, ct.POINTER(vp)]),
         "amrlbm_net_destroy": (ct.c_int, [vp]),
         "amrlbm_net_param_count": (ct.c_int32, []),
@@ -466,7 +467,19 @@ class AmrLbm:
         self._check(self.lib.amrlbm_set_regrid_net(self.ctx, net.h if net else None, horizon,
                                                    threshold))
 
+    def forecast_blocks(self, ids):
+        """Logits of the attached forecaster on blocks ids by the fused kernel
+        of the learned regrid (amrlbm_forecast_blocks)."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        z = np.zeros(len(ids), dtype=np.float32)
+        self._check(self.lib.amrlbm_forecast_blocks(self.ctx, len(ids), _ptr(ids, ct.c_int32),
+                                                    _ptr(z, ct.c_float)))
+        return z
+
     def regrid_stats(self):
+        """amrlbm_regrid_stats since the start-up: regrids, leaves forecast,
+        leaves the criterion flagged (escapes), flagged ones the forecast
+        missed, forecast ones not flagged."""
         a = (ct.c_int64 * 5)()
         self._check(self.lib.amrlbm_regrid_stats(self.ctx, a))
         return dict(zip(("regrids", "forecast", "flagged", "missed", "extra"), list(a)))

@@ -63,7 +63,10 @@ struct amrlbm_ctx {
     // learned regrid (amrlbm_set_regrid_net)
     amrlbm_net* net = nullptr;
     float net_horizon = 16.f, net_logit = 0.f;
-    int64_t rstats[5] = {0, 0, 0, 0, 0};
+    ForecastNet fnet{};
+    float* d_logits = nullptr;  // amrlbm_forecast_blocks: logits and block ids
+    int* d_lids = nullptr;
+    size_t logit_cap = 0;
     float* d_feat = nullptr;
     int* d_fids = nullptr;
     size_t feat_cap = 0;
@@ -311,6 +314,14 @@ struct ProfMark {
     }
 };
 
+// the learned regrid's forecast (a net attached): raises the error of the
+// leaves it forecasts before the refine flags are taken
+void enqueue_forecast(amrlbm_ctx* ctx) {
+    if (ctx->net)
+        launch_forecast(ctx->s, ctx->lc, ctx->st, ctx->fnet, 0, nullptr, nullptr, ctx->net_horizon,
+                        ctx->prm.refin_tol, ctx->net_logit);
+}
+
 // Refine_Derefine_Mesh in a mixed-precision run: the flags from the err that
 // the tail computed, and the FP64 restriction (Restrict.f90, FP64 sums) and
 // prolongation kernels on FP64 copies of just the blocks they read, converted
@@ -345,6 +356,7 @@ void enqueue_step_mp(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail,
     }
     if (regrid) {
         ProfMark m(ctx, ge, 3);
+        enqueue_forecast(ctx);
         enqueue_regrid_mp(ctx, ctx->prm.refin_tol, ctx->prm.deref_tol);
     }
 }
@@ -371,6 +383,7 @@ void enqueue_step(amrlbm_ctx* ctx, GraphEntry* ge, bool prev_tail, bool tail, bo
     }
     if (regrid) {
         ProfMark m(ctx, ge, 3);
+        enqueue_forecast(ctx);
         enqueue_regrid(ctx, ctx->prm.refin_tol, ctx->prm.deref_tol, false, true);
     }
 }
@@ -600,6 +613,8 @@ int amrlbm_destroy(amrlbm_ctx* ctx) {
     if (ctx->d_flush) cudaFree(ctx->d_flush);
     if (ctx->d_feat) cudaFree(ctx->d_feat);
     if (ctx->d_fids) cudaFree(ctx->d_fids);
+    if (ctx->d_logits) cudaFree(ctx->d_logits);
+    if (ctx->d_lids) cudaFree(ctx->d_lids);
     if (ctx->t0) cudaEventDestroy(ctx->t0);
     if (ctx->t1) cudaEventDestroy(ctx->t1);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -1027,10 +1042,18 @@ int amrlbm_init_fields(amrlbm_ctx* ctx) {
 // generalised to nbx x nby blocks (periodic in x, walls in y).
 int init_batch(amrlbm_ctx* ctx);
 
+int init_single(amrlbm_ctx* ctx);
+
 int amrlbm_init_rising_bubble(amrlbm_ctx* ctx) {
     if (!ctx) return AMRLBM_ERR_ARG;
     ensure_fp64(ctx, true);
-    if (ctx->s.n_inst) return init_batch(ctx);
+    if (int r = ctx->s.n_inst ? init_batch(ctx) : init_single(ctx)) return r;
+    // the regrid statistics count from here (not the start-up rounds)
+    CK(cudaMemsetAsync(ctx->s.cnt->rstat, 0, sizeof(ctx->s.cnt->rstat), ctx->st));
+    return sync_check(ctx);
+}
+
+int init_single(amrlbm_ctx* ctx) {
     const amrlbm_params& p = ctx->prm;
     const int nbx = p.nbx, nby = p.nby, nb = nbx * nby;
     // Initialize_Base_Block + Fix_Initial_Neighbors_3Blocks (:79-138)
@@ -1148,8 +1171,6 @@ int amrlbm_regrid(amrlbm_ctx* ctx, double refin_tol, double deref_tol) {
     return sync_check(ctx);
 }
 
-int learned_regrid(amrlbm_ctx* ctx);
-
 int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
     if (!ctx || nsteps < 0) return AMRLBM_ERR_ARG;
     if (nsteps == 0) return AMRLBM_OK;
@@ -1168,7 +1189,6 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
         const bool final_chunk = (done + chunk == nsteps);
         const auto key = std::make_tuple(chunk, phase, ctx->tail_done ? 1 : 0, final_chunk ? 1 : 0,
                                          ctx->prof ? 1 : 0);
-        const bool learned = ctx->net != nullptr;  // the regrid runs after the graph
         if (ctx->prof_pending) {  // the previous replay's events must be read first
             CK(cudaStreamSynchronize(ctx->st));
             harvest_profile(ctx);
@@ -1182,8 +1202,7 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
             for (int t = 0; t < chunk; ++t) {
                 const bool regrid = ((phase + t + 1) % R) == 0;
                 const bool tail = regrid || (final_chunk && t == chunk - 1);
-                enqueue_step(ctx, &ge, prev_tail, tail, regrid && !learned,
-                             (final_chunk && t == chunk - 1) || (regrid && learned));
+                enqueue_step(ctx, &ge, prev_tail, tail, regrid, final_chunk && t == chunk - 1);
                 prev_tail = tail;
             }
             cudaGraph_t g;
@@ -1206,9 +1225,6 @@ int amrlbm_step(amrlbm_ctx* ctx, int32_t nsteps) {
         ctx->stepcount += chunk;
         ctx->tail_done = last_tail;
         done += chunk;
-        if (learned && ctx->stepcount % R == 0) {
-            if (int r = learned_regrid(ctx)) return r;
-        }
     }
     CK(cudaGetLastError());
     return AMRLBM_OK;
@@ -1783,60 +1799,6 @@ int features_to_device(amrlbm_ctx* ctx, int n, const int* ids, float horizon) {
 
 }  // namespace
 
-// Refine_Derefine_Mesh with the forecaster: every leaf that may still refine
-// is refined if the forecaster expects it flagged within its horizon or if
-// the reference's criterion (Err_Interface > refin_tol, Refine_Derefine.f90:
-// 36-40) flags it now; a leaf the criterion flags and the forecaster missed
-// is counted. The forecast enters the regrid as the leaf's error raised to
-// twice the tolerance, which also keeps its parent from derefining.
-int learned_regrid(amrlbm_ctx* ctx) {
-    CK(cudaStreamSynchronize(ctx->st));
-    ensure_fp64(ctx, true);
-    const Counters c = read_counters(ctx);
-    std::vector<int> leaves;
-    HostTopo t;
-    if (int r = get_leaves_host(ctx, leaves, t)) return r;
-    std::vector<int> inst;
-    if (ctx->s.n_inst) {
-        inst.resize(t.dx.size());
-        CK(cudaMemcpy(inst.data(), ctx->s.inst, inst.size() * sizeof(int), cudaMemcpyDeviceToHost));
-    }
-    std::vector<double> err((size_t)c.nblks + 1);
-    CK(cudaMemcpy(err.data(), ctx->s.err, err.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    std::vector<int> cand;
-    for (int n : leaves) {
-        const int mlv = ctx->s.n_inst ? ctx->insts[inst[n]].max_levels : ctx->prm.max_levels;
-        if (t.level[n] < mlv && t.level[n] >= c.level_min && t.level[n] <= c.level_max) cand.push_back(n);
-    }
-    std::vector<float> logit(cand.size());
-    if (int r = features_to_device(ctx, (int)cand.size(), cand.data(), ctx->net_horizon)) return r;
-    if (!cand.empty()) {
-        CK(cudaStreamSynchronize(ctx->st));
-        if (int r = amrlbm_net_forward_device(ctx->net, (int)cand.size(), ctx->d_feat, logit.data()))
-            return fail(ctx, r, "forecaster forward");
-    }
-    const double rt = ctx->prm.refin_tol;
-    int64_t pred = 0, crit = 0, missed = 0, extra = 0;
-    for (size_t i = 0; i < cand.size(); ++i) {
-        const int n = cand[i];
-        const bool p = logit[i] > ctx->net_logit, k = err[n] > rt;
-        pred += p;
-        crit += k;
-        missed += (k && !p);
-        extra += (p && !k);
-        if (p && !k) err[n] = 2.0 * rt;
-    }
-    CK(cudaMemcpy(ctx->s.err, err.data(), err.size() * sizeof(double), cudaMemcpyHostToDevice));
-    enqueue_regrid(ctx, rt, ctx->prm.deref_tol, false, true);
-    ctx->tail_done = true;
-    ctx->rstats[0] += 1;
-    ctx->rstats[1] += pred;
-    ctx->rstats[2] += crit;
-    ctx->rstats[3] += missed;
-    ctx->rstats[4] += extra;
-    return sync_check(ctx);
-}
-
 extern "C" {
 
 int amrlbm_set_bubbles(amrlbm_ctx* ctx, int32_t n, const double* xyr) {
@@ -1868,14 +1830,46 @@ int amrlbm_set_regrid_net(amrlbm_ctx* ctx, amrlbm_net* net, float horizon, float
     ctx->net = net;
     ctx->net_horizon = horizon;
     ctx->net_logit = net ? std::log(threshold / (1.f - threshold)) : 0.f;
+    if (net) ctx->fnet = net_forecast_params(net);
+    ctx->s.forecast = net ? 1 : 0;
     drop_graphs(ctx);
     return AMRLBM_OK;
 }
 
 int amrlbm_regrid_stats(amrlbm_ctx* ctx, int64_t out[5]) {
     if (!ctx || !out) return AMRLBM_ERR_ARG;
-    for (int i = 0; i < 5; ++i) out[i] = ctx->rstats[i];
+    if (int r = sync_check(ctx)) return r;
+    const Counters c = read_counters(ctx);
+    for (int i = 0; i < 5; ++i) out[i] = (int64_t)c.rstat[i];
     return AMRLBM_OK;
+}
+
+int amrlbm_forecast_blocks(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, float* logits) {
+    if (!ctx || n < 0 || (n > 0 && (!ids || !logits))) return AMRLBM_ERR_ARG;
+    if (!ctx->net) return fail(ctx, AMRLBM_ERR_STATE, "no forecaster attached");
+    for (int i = 0; i < n; ++i)
+        if (ids[i] < 1 || ids[i] > ctx->prm.max_blks) return AMRLBM_ERR_ARG;
+    if (n == 0) return AMRLBM_OK;
+    if ((size_t)n > ctx->logit_cap) {
+        if (ctx->d_logits) cudaFree(ctx->d_logits);
+        if (ctx->d_lids) cudaFree(ctx->d_lids);
+        ctx->d_logits = nullptr;
+        ctx->d_lids = nullptr;
+        ctx->logit_cap = 0;
+        CK(cudaMalloc(&ctx->d_logits, (size_t)n * sizeof(float)));
+        CK(cudaMalloc(&ctx->d_lids, (size_t)n * sizeof(int)));
+        ctx->logit_cap = (size_t)n;
+    }
+    if (ctx->s.mp.fmt && ctx->mp_stale) {  // the kernel reads the mixed-precision fields
+        launch_mp_convert(ctx->s, ctx->lc, ctx->st, 0, 1);
+        ctx->mp_stale = false;
+        ctx->fp64_stale = true;
+    }
+    CK(cudaMemcpyAsync(ctx->d_lids, ids, n * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    launch_forecast(ctx->s, ctx->lc, ctx->st, ctx->fnet, n, ctx->d_lids, ctx->d_logits,
+                    ctx->net_horizon, ctx->prm.refin_tol, ctx->net_logit);
+    CK(cudaMemcpyAsync(logits, ctx->d_logits, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    return sync_check(ctx);
 }
 
 }  // extern "C"

@@ -39,6 +39,10 @@ struct Counters {
     int n_alloc_new;                             // refinements that appended new ids
     int n_ref_flag;    // blocks of the level range flagged for refinement by k_regrid_flags
     int topo_changed;  // whether the last k_regrid_topo changed the mesh (plans rebuilt)
+    // regrid statistics (amrlbm_regrid_stats): regrids, leaves forecast,
+    // leaves the criterion flagged, flagged ones not forecast, forecast ones
+    // not flagged
+    unsigned long long rstat[5];
 };
 
 // Work queues of the level-ordered kernels (queue[4q..4q+2]: next fill item,
@@ -115,6 +119,7 @@ struct DevState {
     int *freelist;   // ring buffer of the first ids of freed quartets
     int *ref_list, *ref_c1, *der_list;
     Counters* cnt;
+    int forecast;  // a forecaster runs before each regrid of the time step (it keeps the statistics)
     unsigned* queue;  // [4*NQUEUES]: per queue fill claims, consumer claims, CTAs done
     int spin_limit;   // iterations of a flag wait of the level-ordered fills
     int hold_flag;    // test hook: this block's ring flag is never raised (0: none)

@@ -164,21 +164,30 @@ __global__ void __launch_bounds__(AMR_NTHREADS_TOPO) k_regrid_flags(DevState s, 
     // levels that hold a block flagged for refinement / derefinement: the
     // closure passes of the other levels have nothing to do (each pass only
     // adds flags one level down, after the barrier that ends the pass before)
-    __shared__ unsigned s_rmask, s_dmask;
-    if (threadIdx.x == 0) s_rmask = s_dmask = 0u;
+    __shared__ unsigned s_rmask, s_dmask, s_flagged;
+    if (threadIdx.x == 0) s_rmask = s_dmask = s_flagged = 0u;
     __syncthreads();
     for (int n = 1 + threadIdx.x; n <= nb; n += blockDim.x) {
         uint8_t r = 0;
         if (s.is_leaf[n] && (!s.n_inst || s.inst_active[s.inst[n]])) {
-            if (s.level[n] < s.min_levels)
+            if (s.level[n] < s.min_levels) {
                 r = 1;
-            else if (s.level[n] < maxlv_of(s, n) && s.err[n] > refin_tol)
+            } else if (s.level[n] < maxlv_of(s, n) && s.err[n] > refin_tol) {
                 r = 1;
+                if (s.level[n] >= lmin && s.level[n] <= lmax) atomicAdd(&s_flagged, 1u);
+            }
         }
         s.refin[n] = r;
         if (r) atomicOr(&s_rmask, 1u << s.level[n]);
     }
     __syncthreads();
+    if (threadIdx.x == 0) {  // statistics; with a forecaster it counts the flags itself
+        s.cnt->rstat[0] += 1;
+        if (!s.forecast) {
+            s.cnt->rstat[2] += s_flagged;
+            s.cnt->rstat[3] += s_flagged;
+        }
+    }
     // closure: a refining block's coarser (Level-1) leaf neighbours refine too;
     // processed from fine to coarse, every propagation goes one level down
     for (int L = s.max_levels; L >= 1; --L) {

@@ -81,3 +81,19 @@ void launch_mp_prepare(const DevState& s, const LaunchCfg& lc);
 // parents, 4 their children; to_mp: FP64 -> mixed, else back
 void launch_mp_convert(const DevState& s, const LaunchCfg& lc, cudaStream_t st, int mode,
                        int to_mp);
+
+// the refine-flag forecaster's device parameters (amrlbm_net.cu): BF16
+// weight matrices W1 [48][32] (rows 36.. zero), W2, W3 [288][32], FP32
+// biases, dense weights and bias
+struct ForecastNet {
+    const void *w1, *w2, *w3;
+    const float *b1, *b2, *b3, *wd, *bd;
+};
+struct amrlbm_net;
+ForecastNet net_forecast_params(const amrlbm_net* net);
+// learned regrid (amrlbm_forecast.cu). ids == nullptr: every leaf of the
+// level range that may still refine; a forecast (logit > thr) that the
+// criterion (err > tol) does not flag raises err to 2 tol; statistics into
+// the counters. Else logits[i] of blocks ids[0..n_ids) (device arrays).
+void launch_forecast(const DevState& s, const LaunchCfg& lc, cudaStream_t st, const ForecastNet& net,
+                     int n_ids, const int* ids, float* logits, float horizon, double tol, float thr);

@@ -24,8 +24,8 @@
 #include <vector>
 
 #include "amrlbm.h"
-
-void count_launches(int n);
+#include "amrlbm_dev.cuh"
+#include "amrlbm_launch.h"
 
 namespace {
 
@@ -127,15 +127,16 @@ __global__ void k_input(int n, const float* x, __nv_bfloat16* a) {
         a[i] = __float2bfloat16(x[((long long)b * CIN + c) * PIX + p]);
     }
 }
-// im2col of a channels-last activation [n*PIX][cin]: col[row][k], k = ci*9 + o,
-// o = (dy+1)*3 + (dx+1), zero outside the tile and for k >= cin*9
+// im2col of a channels-last activation [n*PIX][cin]: col[row][k], k = o*cin + ci
+// (tap-major: the 16 columns of one product step are whole taps of adjacent
+// channels), o = (dy+1)*3 + (dx+1), zero outside the tile and for k >= cin*9
 __global__ void k_im2col(int n, int cin, int kp, const __nv_bfloat16* a, __nv_bfloat16* col) {
     GRID_STRIDE(i, (long long)n * PIX * kp) {
         const long long row = i / kp;
         const int k = (int)(i % kp), b = (int)(row / PIX), p = (int)(row % PIX);
         __nv_bfloat16 v = __float2bfloat16(0.f);
         if (k < cin * 9) {
-            const int ci = k / 9, o = k % 9, y = p / TILE + o / 3 - 1, x = p % TILE + o % 3 - 1;
+            const int o = k / cin, ci = k % cin, y = p / TILE + o / 3 - 1, x = p % TILE + o % 3 - 1;
             if (x >= 0 && x < TILE && y >= 0 && y < TILE)
                 v = a[((long long)b * PIX + y * TILE + x) * cin + ci];
         }
@@ -229,7 +230,7 @@ __global__ void k_colsum(long long m, const float* dz, float* out) {
     }
     if (threadIdx.x == 0) out[c] = red[0];
 }
-// col2im: dA[row q][ci] = sum over the 3x3 offsets o of dcol[row q - o][ci*9 + o]
+// col2im: dA[row q][ci] = sum over the 3x3 offsets o of dcol[row q - o][o*cin + ci]
 __global__ void k_col2im(int n, int cin, int kp, const float* dcol, float* dA) {
     GRID_STRIDE(i, (long long)n * PIX * cin) {
         const long long row = i / cin;
@@ -239,7 +240,7 @@ __global__ void k_col2im(int n, int cin, int kp, const float* dcol, float* dA) {
         for (int o = 0; o < 9; ++o) {
             const int py = y - (o / 3 - 1), px = x - (o % 3 - 1);
             if (px >= 0 && px < TILE && py >= 0 && py < TILE)
-                s += dcol[((long long)b * PIX + py * TILE + px) * kp + ci * 9 + o];
+                s += dcol[((long long)b * PIX + py * TILE + px) * kp + o * cin + ci];
         }
         dA[i] = s;
     }
@@ -384,6 +385,19 @@ int load_batch(amrlbm_net* net, int n, const float* x, const float* y) {
 }
 
 }  // namespace
+
+ForecastNet net_forecast_params(const amrlbm_net* net) {
+    ForecastNet f;
+    f.w1 = net->w1;
+    f.w2 = net->w2;
+    f.w3 = net->w3;
+    f.b1 = net->p + O_B1;
+    f.b2 = net->p + O_B2;
+    f.b3 = net->p + O_B3;
+    f.wd = net->p + O_WD;
+    f.bd = net->p + O_BD;
+    return f;
+}
 
 extern "C" {
 

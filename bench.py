@@ -417,15 +417,8 @@ def learned_leg(samples_target=1_000_000, eval_steps=960):
         s = amrlbm.AmrLbm(p2)
         s.set_bubbles(b2)
         s.initialize_rising_bubble()
-        never = None
-        if use:
+        if use:  # the forecast runs inside the step's graph before each regrid
             s.set_regrid_net(net, horizon=16.0, threshold=0.5)
-        else:  # counted through a forecaster that never fires
-            never = amrlbm.Net(seed=7, max_batch=512)
-            q = never.params()
-            q[-1] = -1e4
-            never.set_params(q)
-            s.set_regrid_net(never, horizon=16.0, threshold=0.5)
         c0 = s.profile_read(0)[2]
         s.sync()
         s.timer_start()
@@ -437,8 +430,6 @@ def learned_leg(samples_target=1_000_000, eval_steps=960):
         check_state(s.output(), name)
         out[name] = st
         s.close()
-        if never:
-            never.close()
     net.close()
     return out
 

@@ -326,7 +326,7 @@ int amrlbm_diag_instances(amrlbm_ctx* ctx, double* out);
  * weights and activations on the tensor cores, FP32 accumulation, FP32 master
  * weights trained with Adam on a weighted binary cross-entropy. Parameter
  * vector (amrlbm_net_param_count floats): W1 [36][32], b1, W2 [288][32], b2,
- * W3 [288][32], b3, wd [32], bd, with W[(ci*9 + (dy+1)*3 + (dx+1))][co]. */
+ * W3 [288][32], b3, wd [32], bd, with W[((dy+1)*3 + (dx+1))*c_in + ci][co]. */
 #define AMRLBM_NET_CHANNELS 4
 #define AMRLBM_NET_TILE 18
 typedef struct amrlbm_net amrlbm_net;
@@ -365,12 +365,22 @@ int amrlbm_block_features(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, float 
  * leaves the forecaster flags (probability > threshold; its samples taken
  * with `horizon`) together with those the reference's criterion
  * (Err_Interface > refin_tol) flags; NULL restores the criterion alone. The
- * net must outlive its use. stats (accumulated over the context's life):
- * [0] regrids, [1] leaves forecast, [2] leaves the criterion flagged,
- * [3] flagged leaves the forecast missed (refined all the same), [4] leaves
+ * forecast runs on the device inside the step's graph, one fused kernel over
+ * the leaves that may still refine, with the net's current weights (training
+ * after this call is seen by later regrids). The net must outlive its use.
+ * stats of the regrids of amrlbm_step and amrlbm_refine_derefine_mesh since
+ * the start-up (amrlbm_init_rising_bubble resets them): [0] regrids, [1]
+ * leaves forecast, [2] leaves the criterion flagged (leaves of the level
+ * range that may still refine), [3] flagged leaves the forecast missed
+ * (refined all the same; without a net every flagged leaf), [4] leaves
  * forecast but not flagged. */
 int amrlbm_set_regrid_net(amrlbm_ctx* ctx, amrlbm_net* net, float horizon, float threshold);
 int amrlbm_regrid_stats(amrlbm_ctx* ctx, int64_t out[5]);
+/* logits[i] of the attached net (amrlbm_set_regrid_net) on block ids[i] of
+ * the current state by the fused kernel of the learned regrid: equal, bit
+ * for bit, to amrlbm_net_forward on amrlbm_block_features of the same
+ * blocks. */
+int amrlbm_forecast_blocks(amrlbm_ctx* ctx, int32_t n, const int32_t* ids, float* logits);
 /* Several bubbles for amrlbm_init_rising_bubble / amrlbm_init_fields (n
  * triples x, y, R in finest cells; n = 0: the params' one bubble): C is the
  * tanh profile of the nearest bubble's surface, P as for one bubble with the

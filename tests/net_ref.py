@@ -30,23 +30,23 @@ def bf16(a):
 
 
 def im2col(a):
-    """[n, H, W, c] -> [n, H, W, c*9], column ci*9 + (dy+1)*3 + (dx+1)."""
+    """[n, H, W, c] -> [n, H, W, 9*c], column o*c + ci, o = (dy+1)*3 + (dx+1)."""
     n, H, W, c = a.shape
     ap = np.pad(a, ((0, 0), (1, 1), (1, 1), (0, 0)))
-    cols = np.zeros((n, H, W, c, 9))
+    cols = np.zeros((n, H, W, 9, c))
     for o in range(9):
         dy, dx = o // 3 - 1, o % 3 - 1
-        cols[..., o] = ap[:, 1 + dy:1 + dy + H, 1 + dx:1 + dx + W, :]
-    return cols.reshape(n, H, W, c * 9)
+        cols[..., o, :] = ap[:, 1 + dy:1 + dy + H, 1 + dx:1 + dx + W, :]
+    return cols.reshape(n, H, W, 9 * c)
 
 
 def col2im(dcol, c):
     n, H, W, _ = dcol.shape
-    d = dcol.reshape(n, H, W, c, 9)
+    d = dcol.reshape(n, H, W, 9, c)
     out = np.zeros((n, H + 2, W + 2, c))
     for o in range(9):
         dy, dx = o // 3 - 1, o % 3 - 1
-        out[:, 1 + dy:1 + dy + H, 1 + dx:1 + dx + W, :] += d[..., o]
+        out[:, 1 + dy:1 + dy + H, 1 + dx:1 + dx + W, :] += d[..., o, :]
     return out[:, 1:H + 1, 1:W + 1, :]
 
 

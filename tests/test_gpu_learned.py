@@ -52,6 +52,50 @@ def test_features_are_the_fields():
     g.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp16"])
+def test_fused_forecast_equals_the_network(precision):
+    """The learned regrid's fused kernel (features from the pool, three
+    convolutions on the tensor cores, max pool, dense output in one launch)
+    gives the unfused network's logits on the same samples: bit for bit in
+    FP64 storage; with FP16 storage it reads the FP32 fields, so the samples
+    (and logits) differ from the FP64 copy's by storage rounding only."""
+    g = _sim(4)
+    g.main_loop(40)
+    net = Net(seed=5, max_batch=256)
+    p = net.params()
+    rng = np.random.default_rng(9)
+    p[:] = p + 0.05 * rng.standard_normal(p.shape).astype(np.float32)
+    net.set_params(p)
+    g.set_regrid_net(net, horizon=16.0, threshold=0.5)
+    if precision != "fp64":
+        g.set_precision(precision)
+        g.main_loop(4)
+    ids = g.leaves()
+    z_fused = g.forecast_blocks(ids)
+    x = g.block_features(ids, 16.0)
+    z_ref = net.forward(x)
+    assert np.all(np.isfinite(z_fused)) and np.std(z_ref) > 0
+    if precision == "fp64":
+        assert np.array_equal(z_fused, z_ref)
+    else:
+        assert np.allclose(z_fused, z_ref, rtol=2e-2, atol=2e-2 * np.abs(z_ref).max())
+    g.set_regrid_net(None)
+    g.close()
+    net.close()
+
+
+def test_regrid_statistics_without_a_net():
+    """The criterion alone counts its regrids and flagged leaves (every one
+    of them an escape: nothing forecast it)."""
+    g = _sim(6, regrid_every=64)
+    assert g.regrid_stats() == {"regrids": 0, "forecast": 0, "flagged": 0, "missed": 0, "extra": 0}
+    g.main_loop(64 * 4)
+    st = g.regrid_stats()
+    assert st["regrids"] == 4 and st["forecast"] == 0 and st["extra"] == 0
+    assert st["missed"] == st["flagged"]
+    g.close()
+
+
 def test_learned_regrid_flags_fewer_escapes_than_the_criterion_alone():
     """Regrids 256 steps apart, forecast horizon 128: with 16x16 blocks the
     refined region holds the interface for tens of steps (at the default
@@ -74,15 +118,11 @@ def test_learned_regrid_flags_fewer_escapes_than_the_criterion_alone():
     losses = amrlbm.train_net(net, x, y, epochs=20, batch=128, lr=2e-3)
     z = net.forward(x.astype(np.float32))
     recall = float(((z > 0) & (y > 0)).sum() / max(y.sum(), 1))
-    # the criterion alone, counted the same way: a forecaster that never fires
-    never = Net(seed=7, max_batch=512)
-    p = never.params()
-    p[-1] = -1e4  # output bias: probability 0
-    never.set_params(p)
     res = {}
-    for name, n in (("criterion", never), ("learned", net)):
+    for name, n in (("criterion", None), ("learned", net)):
         s = _sim(23, regrid_every=R)
-        s.set_regrid_net(n, horizon=float(H), threshold=0.5)
+        if n is not None:
+            s.set_regrid_net(n, horizon=float(H), threshold=0.5)
         s.main_loop(R * 16)
         res[name] = s.regrid_stats()
         res[name]["leaves"] = s.counts()["nleaf"]
@@ -100,4 +140,3 @@ def test_learned_regrid_flags_fewer_escapes_than_the_criterion_alone():
     assert res["learned"]["flagged"] < res["criterion"]["flagged"]
     assert res["learned"]["missed"] <= res["learned"]["flagged"]
     net.close()
-    never.close()
