@@ -40,6 +40,7 @@ struct Smem {
     __nv_bfloat16 act[2][PIX][AROW];
     float b[3][CH], wd[CH], bd;
     float pmax[NWARP][CH];
+    __align__(16) unsigned zero[4];  // the operand row outside the tile
 };
 
 __device__ __forceinline__ unsigned pack2(float lo, float hi) {
@@ -89,25 +90,99 @@ __device__ __forceinline__ void tile_product(const unsigned* act, const __nv_bfl
     }
 }
 
-// hidden layer: ReLU(product + bias) as BF16 into the next activation
-template <int CI, int AW, int K, int KW>
-__device__ __forceinline__ void hidden_layer(const unsigned* in, const __nv_bfloat16 (*wt)[KW],
-                                             const float* bias, __nv_bfloat16 (*out)[AROW], int warp,
-                                             int g, int q) {
+// ReLU(acc + bias) of one row tile as BF16 into an activation
+__device__ __forceinline__ void store_tile(const float acc[4][4], const float* bias, unsigned* o32,
+                                           int mt, int g, int q) {
+    const int r0 = 16 * mt + g, r1 = r0 + 8;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int n = 8 * j + 2 * q;
+        if (r0 < PIX)
+            o32[r0 * (AROW / 2) + (n >> 1)] =
+                pack2(fmaxf(acc[j][0] + bias[n], 0.f), fmaxf(acc[j][1] + bias[n + 1], 0.f));
+        if (r1 < PIX)
+            o32[r1 * (AROW / 2) + (n >> 1)] =
+                pack2(fmaxf(acc[j][2] + bias[n], 0.f), fmaxf(acc[j][3] + bias[n + 1], 0.f));
+    }
+}
+
+// the first layer (4 input channels: one 16-column step spans four taps):
+// operands gathered pair by pair
+__device__ __forceinline__ void first_layer(const unsigned* x0, const __nv_bfloat16 (*wt)[KW1],
+                                            const float* bias, __nv_bfloat16 (*out)[AROW], int warp,
+                                            int g, int q) {
     unsigned* o32 = reinterpret_cast<unsigned*>(out);
     for (int mt = warp; mt < MTILES; mt += NWARP) {
         float acc[4][4];
-        tile_product<CI, AW, K, KW>(in, wt, mt, g, q, acc);
-        const int r0 = 16 * mt + g, r1 = r0 + 8;
+        tile_product<CIN, CIN / 2, K1P, KW1>(x0, wt, mt, g, q, acc);
+        store_tile(acc, bias, o32, mt, g, q);
+    }
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void ldsm4(unsigned addr, unsigned& r0, unsigned& r1, unsigned& r2,
+                                      unsigned& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+
+// a 32-channel layer: each 16-column step is one tap of 16 adjacent
+// channels, so the operand fragments come by ldmatrix: A rows are the
+// activation rows of the shifted pixels (a zero row outside the tile), B the
+// transposed weights. The warp's row tiles mt = warp, warp + 8, warp + 16
+// share each step's B fragments. Accumulation order along K as k_gemm's.
+template <int KW>
+__device__ __forceinline__ void conv32(const __nv_bfloat16 (*act)[AROW], const __nv_bfloat16 (*wt)[KW],
+                                       unsigned zero_row, int warp, int lane, float acc[3][4][4]) {
+    const int lr = lane & 15;
+    int pix[3];
+    unsigned vmask[3];  // bit o: tap o of this lane's row lies in the tile
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int n = 8 * j + 2 * q;
-            if (r0 < PIX)
-                o32[r0 * (AROW / 2) + (n >> 1)] =
-                    pack2(fmaxf(acc[j][0] + bias[n], 0.f), fmaxf(acc[j][1] + bias[n + 1], 0.f));
-            if (r1 < PIX)
-                o32[r1 * (AROW / 2) + (n >> 1)] =
-                    pack2(fmaxf(acc[j][2] + bias[n], 0.f), fmaxf(acc[j][3] + bias[n + 1], 0.f));
+    for (int u = 0; u < 3; ++u) {
+        const int r = 16 * (warp + NWARP * u) + lr;
+        pix[u] = r;
+        vmask[u] = 0u;
+        if (r < PIX) {
+            const int y = r / TILE, x = r % TILE;
+#pragma unroll
+            for (int o = 0; o < 9; ++o) {
+                const int yy = y + o / 3 - 1, xx = x + o % 3 - 1;
+                if (yy >= 0 && yy < TILE && xx >= 0 && xx < TILE) vmask[u] |= 1u << o;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[u][j][i] = 0.f;
+    }
+    const unsigned abase = smem_addr(&act[0][0]) + (unsigned)((lane >> 4) * 8 * 2);
+    const unsigned bbase = smem_addr(&wt[(lane & 7) + ((lane >> 4) << 3)][((lane >> 3) & 1) * 8]);
+    const bool third = warp + 2 * NWARP < MTILES;
+#pragma unroll
+    for (int c = 0; c < K2 / 16; ++c) {
+        const int o = c >> 1, c0 = (c & 1) * 16;
+        const int shift = (o / 3 - 1) * TILE + (o % 3 - 1);
+        unsigned b[8];
+        ldsm4(bbase + (unsigned)(c * 32), b[0], b[1], b[2], b[3]);                    // n 0..15
+        ldsm4(bbase + (unsigned)(16 * KW * 2 + c * 32), b[4], b[5], b[6], b[7]);      // n 16..31
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            if (u == 2 && !third) break;
+            const unsigned addr = ((vmask[u] >> o) & 1u)
+                                      ? abase + (unsigned)(((pix[u] + shift) * AROW + c0) * 2)
+                                      : zero_row;
+            unsigned a0, a1, a2, a3;
+            ldsm4(addr, a0, a1, a2, a3);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                asm volatile(
+                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+                    "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                    : "+f"(acc[u][j][0]), "+f"(acc[u][j][1]), "+f"(acc[u][j][2]), "+f"(acc[u][j][3])
+                    : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b[2 * j]), "r"(b[2 * j + 1]));
         }
     }
 }
@@ -135,7 +210,9 @@ __global__ void __launch_bounds__(NT, 2)
             S.wd[t] = net.wd[t];
         }
         if (t == 0) S.bd = net.bd[0];
+        if (t < 4) S.zero[t] = 0u;
     }
+    const unsigned zero_row = smem_addr(S.zero);
     const bool explicit_ids = ids != nullptr;
     const int total = explicit_ids ? n_ids : s.cnt->nleaf;
     const int lmin = s.cnt->level_min, lmax = s.cnt->level_max;
@@ -181,31 +258,41 @@ __global__ void __launch_bounds__(NT, 2)
             x32[1] = pack2(f2, f3);
         }
         __syncthreads();
-        hidden_layer<CIN, CIN / 2, K1P, KW1>(reinterpret_cast<const unsigned*>(S.x0), S.w1, S.b[0],
-                                             S.act[0], warp, g, q);
+        first_layer(reinterpret_cast<const unsigned*>(S.x0), S.w1, S.b[0], S.act[0], warp, g, q);
         __syncthreads();
-        hidden_layer<CH, AROW / 2, K2, KW2>(reinterpret_cast<const unsigned*>(S.act[0]), S.w2, S.b[1],
-                                            S.act[1], warp, g, q);
+        {
+            float acc[3][4][4];
+            conv32<KW2>(S.act[0], S.w2, zero_row, warp, lane, acc);
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                if (warp + NWARP * u < MTILES)
+                    store_tile(acc[u], S.b[1], reinterpret_cast<unsigned*>(S.act[1]), warp + NWARP * u,
+                               g, q);
+        }
         __syncthreads();
         // layer 3 reduced to the channel maxima (global max pool)
         float mx[4][2];
 #pragma unroll
         for (int j = 0; j < 4; ++j) mx[j][0] = mx[j][1] = -1.f;
-        for (int mt = warp; mt < MTILES; mt += NWARP) {
-            float acc[4][4];
-            tile_product<CH, AROW / 2, K2, KW2>(reinterpret_cast<const unsigned*>(S.act[1]), S.w3,
-                                                mt, g, q, acc);
-            const int r0 = 16 * mt + g, r1 = r0 + 8;
+        {
+            float acc[3][4][4];
+            conv32<KW2>(S.act[1], S.w3, zero_row, warp, lane, acc);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int n2 = 8 * j + 2 * q;
-                if (r0 < PIX) {
-                    mx[j][0] = fmaxf(mx[j][0], fmaxf(acc[j][0] + S.b[2][n2], 0.f));
-                    mx[j][1] = fmaxf(mx[j][1], fmaxf(acc[j][1] + S.b[2][n2 + 1], 0.f));
-                }
-                if (r1 < PIX) {
-                    mx[j][0] = fmaxf(mx[j][0], fmaxf(acc[j][2] + S.b[2][n2], 0.f));
-                    mx[j][1] = fmaxf(mx[j][1], fmaxf(acc[j][3] + S.b[2][n2 + 1], 0.f));
+            for (int u = 0; u < 3; ++u) {
+                const int mt = warp + NWARP * u;
+                if (mt >= MTILES) continue;
+                const int r0 = 16 * mt + g, r1 = r0 + 8;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int n2 = 8 * j + 2 * q;
+                    if (r0 < PIX) {
+                        mx[j][0] = fmaxf(mx[j][0], fmaxf(acc[u][j][0] + S.b[2][n2], 0.f));
+                        mx[j][1] = fmaxf(mx[j][1], fmaxf(acc[u][j][1] + S.b[2][n2 + 1], 0.f));
+                    }
+                    if (r1 < PIX) {
+                        mx[j][0] = fmaxf(mx[j][0], fmaxf(acc[u][j][2] + S.b[2][n2], 0.f));
+                        mx[j][1] = fmaxf(mx[j][1], fmaxf(acc[u][j][3] + S.b[2][n2 + 1], 0.f));
+                    }
                 }
             }
         }

@@ -430,8 +430,55 @@ def learned_leg(samples_target=1_000_000, eval_steps=960):
         check_state(s.output(), name)
         out[name] = st
         s.close()
-    net.close()
-    return out
+    return out, net
+
+
+def combined_leg(net, count=256, steps=320, ctas_per_sm=0):
+    """The three layers together on the seeded 256-problem batch: FP16
+    storage, every instance in one pool and one graph per interval, the
+    learned regrid every 32 steps (the forecaster of the learned-regrid leg);
+    against the plain FP64 path on the same batch with the criterion every 10
+    steps. Both run `steps` steps from the start-up, device-timed; per
+    instance, the relative mass and rise-velocity differences at the end."""
+    import numpy as np
+    import amrlbm
+    insts = amrlbm.batch_instances(count)
+    res = {"instances": count, "steps": steps}
+    ends = {}
+    for name, prec, every, use in (("fp64_criterion_every_10", "fp64", 10, False),
+                                   ("fp16_learned_every_32", "fp16", 32, True)):
+        g = amrlbm.AmrLbm(amrlbm.batch_params(n=16, max_blks=400000, regrid_every=every),
+                          instances=insts)
+        g.initialize_rising_bubble()
+        if prec != "fp64":
+            g.set_precision(prec)
+            g.set_launch(ctas_per_sm)
+        if use:
+            g.set_regrid_net(net, horizon=16.0, threshold=0.5)
+        c0 = g.profile_read(0)[2]
+        g.sync()
+        g.timer_start()
+        g.main_loop(steps)
+        ms = g.timer_stop()
+        st = g.regrid_stats()
+        st["mlups"] = (g.profile_read(0)[2] - c0) / (ms / 1e3) / 1e6
+        st["leaves"] = g.counts()["nleaf"]
+        d = g.output_instances()
+        bad = [i for i, x in enumerate(d) if not (x["u_max"] < U_BOUND and x["rho_min"] > 0)]
+        if bad:
+            raise RuntimeError(f"{name}: instances {bad[:8]} not physical")
+        ends[name] = d
+        res[name] = st
+        g.close()
+    a, b = ends["fp64_criterion_every_10"], ends["fp16_learned_every_32"]
+    dm = np.array([abs(y["mass"] - x["mass"]) / abs(x["mass"]) for x, y in zip(a, b)])
+    dv = np.array([abs(y["rise_velocity"] - x["rise_velocity"]) / max(abs(x["rise_velocity"]), 1e-300)
+                   for x, y in zip(a, b)])
+    res["mass_rel_diff"] = {"max": float(dm.max()), "median": float(np.median(dm))}
+    res["rise_velocity_rel_diff"] = {"max": float(dv.max()), "median": float(np.median(dv)),
+                                     "instances_within_1pct": int((dv <= 0.01).sum())}
+    res["speedup"] = res["fp16_learned_every_32"]["mlups"] / res["fp64_criterion_every_10"]["mlups"]
+    return res
 
 
 def run_own(args):
@@ -606,11 +653,13 @@ def run_own(args):
                 "sample": f"the next {chunks4} x {inner} time steps ({el4:.1f} s) at 4 threads, "
                           f"the reference's OMP_NUM_THREADS"}
         orc.close()
-    mixed_err = batched = learned = None
+    mixed_err = batched = learned = combined = None
     if not args.no_mixed:
         mixed_err = mixed_error_report()
         batched = batched_leg()
-        learned = learned_leg()
+        learned, net = learned_leg()
+        combined = combined_leg(net, ctas_per_sm=(batched["autotune"]["best"] or {}).get("ctas_per_sm", 0))
+        net.close()
     line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -620,7 +669,7 @@ def run_own(args):
             "e2e": e2e, "clocks": clk,
             "gpu_launches": int(launches), "kernels": kernels,
             "mixed_precision": mixed or None, "mixed_precision_error": mixed_err,
-            "batched": batched, "learned_regrid": learned,
+            "batched": batched, "learned_regrid": learned, "combined": combined,
             "leaf_cells_per_step": updates / (args.steps * inner),
             "diagnostics": {k: diag[k] for k in ("mass", "y_centroid", "rise_velocity")}}
     print(json.dumps(line), flush=True)
