@@ -693,17 +693,6 @@ __device__ __forceinline__ unsigned macro_g_cell_f(const DevState& s, const Geo<
     dc = a * a + b * b;
     return dv.bad;
 }
-#ifndef AMR_SAFE_OUTLINE
-#define AMR_SAFE_OUTLINE 0
-#endif
-// the IEEE-division collision of one cell, out of line: the rare cells that
-// take it do not put a second copy of the collision body in the hot loop
-template <bool FUSED, bool SHH, bool SHG, int N, bool BGK, bool BATCH>
-__device__ __noinline__ void collide_cell_ieee(const DevState* s, const Geo<N> G, int n, int c,
-                                               double inv_dx, const double* T, const double* Hb,
-                                               const double* Gb) {
-    collide_cell<true, FUSED, SHH, SHG, N, BGK, BATCH>(*s, G, n, c, inv_dx, T, Hb, Gb);
-}
 // Collision of every cell of block n: the branch-free exact division path,
 // and the IEEE path for a cell whose flag says a quotient left its range.
 // SHH, SHG: Hb, Gb point to shared memory (else to memory)
@@ -712,12 +701,8 @@ __device__ __forceinline__ void collide_block(const DevState& s, const Geo<N>& G
                                               const double* T, const double* Hb, const double* Gb) {
     const double inv_dx = 1.0 / (double)__ldg(s.dx + n);  // dx is a power of two: exact
     for (int c = threadIdx.x; c < G.nx * G.ny; c += blockDim.x)
-        if (collide_cell<false, FUSED, SHH, SHG, N, BGK, BATCH>(s, G, n, c, inv_dx, T, Hb, Gb)) {
-            if (AMR_SAFE_OUTLINE)
-                collide_cell_ieee<FUSED, SHH, SHG, N, BGK, BATCH>(&s, G, n, c, inv_dx, T, Hb, Gb);
-            else
-                collide_cell<true, FUSED, SHH, SHG, N, BGK, BATCH>(s, G, n, c, inv_dx, T, Hb, Gb);
-        }
+        if (collide_cell<false, FUSED, SHH, SHG, N, BGK, BATCH>(s, G, n, c, inv_dx, T, Hb, Gb))
+            collide_cell<true, FUSED, SHH, SHG, N, BGK, BATCH>(s, G, n, c, inv_dx, T, Hb, Gb);
 }
 
 // Macroscopic_Values_g_AMR of every cell of block n; returns this thread's
@@ -802,47 +787,53 @@ __device__ void bounce_back_staged(const DevState& s, const Geo<N>& G, int n, bo
 // LBM_Subroutines.f90:41-90) of every cell of block n into B, and
 // Macroscopic_Values_h_AMR (:193-201), from As: the block's h and g planes
 // (ring included) in shared memory, each field 9 planes in the pool layout.
+// streaming coefficients of block n (dt/dx = 1/dx): Perfect_Shift_AMR where
+// the Courant number exceeds 0.9, else Lax-Wendroff with cA, cB, cC
+struct StreamCoef {
+    double cA, cB, cC;
+    bool shift;
+    __device__ __forceinline__ StreamCoef(const DevState& s, int n) {
+        const double cfl = 1.0 / (double)__ldg(s.dx + n);
+        shift = cfl > (double)0.9f;
+        cA = cfl / 2.0 * (1.0 + cfl);
+        cB = 1.0 - cfl * cfl;
+        cC = cfl / 2.0 * (1.0 - cfl);
+    }
+};
+template <int N>
+__device__ __forceinline__ void stream_cell(const DevState& s, const Geo<N>& G, int n, const double* As,
+                                            const StreamCoef& k, int x, int y) {
+    const int FP = 9 * G.aplane;
+    double csum = 0.0;
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        const double* Af = As + f * FP;
+        double* B = f ? s.Bg : s.Bh;
+#pragma unroll
+        for (int i = 1; i <= 9; ++i) {
+            double v;
+            if (i == 1) {
+                v = Af[G.a(0, 1, x, y)];
+            } else if (k.shift) {
+                v = Af[G.a(0, i, x - d_ex(i), y - d_ey(i))];
+            } else {
+                v = k.cA * Af[G.a(0, i, x - d_ex(i), y - d_ey(i))] + k.cB * Af[G.a(0, i, x, y)] -
+                    k.cC * Af[G.a(0, i, x + d_ex(i), y + d_ey(i))];
+            }
+            B[G.bb(n, i, x, y)] = v;
+            if (f == 0) csum = csum + v;
+        }
+    }
+    s.C[G.c(n, x, y)] = csum;
+}
 template <int N>
 __device__ void stream_block(const DevState& s, const Geo<N>& G, int n, const double* As) {
-    const int nx = G.nx, ny = G.ny;
-    const int FP = 9 * G.aplane;
-    const double cfl = 1.0 / (double)__ldg(s.dx + n);
-    const bool shift = cfl > (double)0.9f;
-    const double cA = cfl / 2.0 * (1.0 + cfl), cB = 1.0 - cfl * cfl, cC = cfl / 2.0 * (1.0 - cfl);
-    for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
-        const int x = c % nx + 1, y = c / nx + 1;
-        double csum = 0.0;
-#pragma unroll
-        for (int f = 0; f < 2; ++f) {
-            const double* Af = As + f * FP;
-            double* B = f ? s.Bg : s.Bh;
-#pragma unroll
-            for (int i = 1; i <= 9; ++i) {
-                double v;
-                if (i == 1) {
-                    v = Af[G.a(0, 1, x, y)];
-                } else if (shift) {
-                    v = Af[G.a(0, i, x - d_ex(i), y - d_ey(i))];
-                } else {
-                    v = cA * Af[G.a(0, i, x - d_ex(i), y - d_ey(i))] + cB * Af[G.a(0, i, x, y)] -
-                        cC * Af[G.a(0, i, x + d_ex(i), y + d_ey(i))];
-                }
-                B[G.bb(n, i, x, y)] = v;
-                if (f == 0) csum = csum + v;
-            }
-        }
-        s.C[G.c(n, x, y)] = csum;
-    }
+    const StreamCoef k(s, n);
+    for (int c = threadIdx.x; c < G.nx * G.ny; c += blockDim.x)
+        stream_cell<N>(s, G, n, As, k, c % G.nx + 1, c / G.nx + 1);
 }
-
-#ifndef AMR_K1_MINB
-#define AMR_K1_MINB 2
-#endif
-#ifndef AMR_K1_STAGE
-#define AMR_K1_STAGE 2
-#endif
 __host__ __device__ constexpr int fill_c_min_blocks(int consumer) {
-    return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) ? AMR_K1_MINB : 3;
+    return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) ? 2 : 3;
 }
 
 // Without level order: an item's C ring (block r.n; plan words pl, ring
@@ -891,11 +882,10 @@ __device__ void fast_ring_hg(const DevState& s, const Geo<N>& G, const int* pl, 
 // values, and without level order each stage's plan words and foreign
 // records (copied with the stage's tile).
 __host__ __device__ constexpr bool stage_h(int consumer) {
-    return (consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) && AMR_K1_STAGE >= 2;
+    return consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED;
 }
 __host__ __device__ constexpr bool stage_g(int consumer) {
-    return ((consumer == CONS_COLLIDE_READ || consumer == CONS_COLLIDE_FUSED) && AMR_K1_STAGE >= 1) ||
-           consumer == CONS_MACRO_G;
+    return stage_h(consumer) || consumer == CONS_MACRO_G;
 }
 // doubles of one stage: C tile, h planes, g planes
 __host__ __device__ inline size_t stage_doubles(int cplane, int bplane, int consumer) {
