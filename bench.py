@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision, error-report and batched legs")
+    ap.add_argument("--profile-forecast", action="store_true",
+                    help="profiling mode: the learned regrid's forecast on a reduced learned "
+                         "workload (base 256x512, 4 bubbles), --steps regrid intervals of 32")
     ap.add_argument("--profile-precision", default=None, choices=["fp64", "fp16", "bf16"],
                     help="profiling mode: the workload in this precision for --warmup + "
                          "--steps intervals, nothing else")
@@ -712,10 +715,35 @@ def run_profile(args):
     return 0
 
 
+def run_profile_forecast(args):
+    """The forecast kernel on the learned workload reduced to a 256x512 base
+    (4 bubbles R 32 to 128, 3 levels): a seeded net, regrids every 32 steps,
+    warm-up and timed intervals."""
+    import amrlbm
+    p, b = amrlbm.learned_workload(256, 512, 3, 4, regrid_every=32)
+    if args.max_blks:
+        p.max_blks = args.max_blks
+    g = amrlbm.AmrLbm(p)
+    g.set_bubbles(b)
+    g.initialize_rising_bubble()
+    net = amrlbm.Net(seed=7, max_batch=64)
+    g.set_regrid_net(net, horizon=16.0, threshold=0.5)
+    g.main_loop(32 * args.warmup)
+    v = amrlbm.time_intervals(g, args.steps, 32)
+    check_state(g.output(), "forecast profile run")
+    print(json.dumps({"profile_forecast": True, "leaves": g.counts()["nleaf"], "mlups": v,
+                      "regrid_stats": g.regrid_stats()}), flush=True)
+    g.close()
+    net.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_forecast:
+        return run_profile_forecast(args)
     if args.profile_precision:
         return run_profile(args)
     return run_own(args)
