@@ -436,6 +436,34 @@ def learned_leg(samples_target=1_000_000, eval_steps=960):
     return out, net
 
 
+def long_run_leg(steps=5000):
+    """The headline workload's full 5000 steps from the start-up, device-timed
+    with every regrid and mesh change inside: MLUPS over the whole run, the
+    leaf count along it and the final diagnostics."""
+    import amrlbm
+    p = workload()
+    g = amrlbm.AmrLbm(p)
+    g.initialize_rising_bubble()
+    out = {"steps": steps, "leaves_start": g.counts()["nleaf"]}
+    c0 = g.profile_read(0)[2]
+    ms, done, leaves = 0.0, 0, []
+    while done < steps:
+        k = min(500, steps - done)
+        g.sync()
+        g.timer_start()
+        g.main_loop(k)
+        ms += g.timer_stop()
+        done += k
+        leaves.append(g.counts()["nleaf"])
+    d = g.output()
+    check_state(d, "5000-step run")
+    out.update({"mlups": (g.profile_read(0)[2] - c0) / (ms / 1e3) / 1e6, "ms": ms,
+                "leaves_every_500_steps": leaves,
+                "diagnostics": {k: d[k] for k in ("mass", "u_max", "y_centroid", "rise_velocity")}})
+    g.close()
+    return out
+
+
 def combined_leg(net, count=256, steps=320, ctas_per_sm=0):
     """The three layers together on the seeded 256-problem batch: FP16
     storage, every instance in one pool and one graph per interval, the
@@ -657,6 +685,7 @@ def run_own(args):
                           f"the reference's OMP_NUM_THREADS"}
         orc.close()
     mixed_err = batched = learned = combined = None
+    long_run = long_run_leg()
     if not args.no_mixed:
         mixed_err = mixed_error_report()
         batched = batched_leg()
@@ -673,6 +702,7 @@ def run_own(args):
             "gpu_launches": int(launches), "kernels": kernels,
             "mixed_precision": mixed or None, "mixed_precision_error": mixed_err,
             "batched": batched, "learned_regrid": learned, "combined": combined,
+            "long_run": long_run,
             "leaf_cells_per_step": updates / (args.steps * inner),
             "diagnostics": {k: diag[k] for k in ("mass", "y_centroid", "rise_velocity")}}
     print(json.dumps(line), flush=True)
