@@ -74,6 +74,12 @@ __device__ __forceinline__ unsigned short enc_sr(float v, unsigned salt) {
         return __half_as_ushort(__float2half_rz(v + copysignf((float)(r >> 8) * 3.5527136788e-15f, v)));
     return __half_as_ushort(__float2half_rz(__uint_as_float(b + (r & 0x1fffu))));
 }
+// mass_encode: the eight deviations of a cell's h populations are rounded
+// one after the other, each with the rounding error of the ones before it
+// subtracted (error diffusion within the cell). Their sum, the cell's share
+// of C and of the phase mass, then carries only the last rounding error
+// instead of the sum of eight independent ones.
+
 // FP64 -> FP32 the same way (29 dropped mantissa bits)
 __device__ __forceinline__ float f32_sr(double d, unsigned salt) {
     const unsigned long long b = (unsigned long long)__double_as_longlong(d);
@@ -159,10 +165,14 @@ __device__ __forceinline__ void enc_a9(const MpState& m, const Geo<N>& G, int f,
     (f ? m.A1g : m.A1h)[off - (size_t)8 * G.aplane * n] = v[0];
     unsigned short* D = (f ? m.Adg : m.Adh) + off;
     const float sc = f ? m.sg : m.sh;
+    float e = 0.f;  // h: rounding error carried (mass_encode)
 #pragma unroll
-    for (int q = 2; q <= 9; ++q)
-        D[(size_t)(q - 1) * G.aplane] =
-            enc_sr<FMT>((v[q - 1] - rq(q) * v[0]) * sc, (unsigned)(off + (size_t)(q - 1) * G.aplane) * 2u + f);
+    for (int q = 2; q <= 9; ++q) {
+        const float x = (v[q - 1] - rq(q) * v[0]) * sc - e;
+        const unsigned short w = enc_sr<FMT>(x, (unsigned)(off + (size_t)(q - 1) * G.aplane) * 2u + f);
+        D[(size_t)(q - 1) * G.aplane] = w;
+        if (f == 0) e = dec<FMT>(w) - x;
+    }
 }
 
 // Biquadratic_from_Fine / _Coarse (Interpolations.f90:2-138) of a plan entry
@@ -416,9 +426,14 @@ __device__ __forceinline__ void enc_b9(const MpState& m, const Geo<N>& G, int f,
     (f ? m.B1g : m.B1h)[(size_t)n * G.bplane + c] = v[0];
     unsigned short* D = f ? m.Bdg : m.Bdh;
     const float sc = f ? m.sg : m.sh;
+    float e = 0.f;  // h: rounding error carried (mass_encode)
 #pragma unroll
-    for (int q = 2; q <= 9; ++q)
-        D[G.bb(n, q, x, y)] = enc_sr<FMT>((v[q - 1] - rq(q) * v[0]) * sc, (unsigned)G.bb(n, q, x, y) * 2u + f + 0x9e3779b9u);
+    for (int q = 2; q <= 9; ++q) {
+        const float xv = (v[q - 1] - rq(q) * v[0]) * sc - e;
+        const unsigned short w = enc_sr<FMT>(xv, (unsigned)G.bb(n, q, x, y) * 2u + f + 0x9e3779b9u);
+        D[G.bb(n, q, x, y)] = w;
+        if (f == 0) e = dec<FMT>(w) - xv;
+    }
 }
 
 // ---- K1: Fill_Ghost_Cells_C2 + Symmetric_C2 + collision ----------------------
@@ -953,19 +968,25 @@ __global__ void __launch_bounds__(256) k_mp_convert(const __grid_constant__ DevS
                 // each rounded once, at random (see enc_sr)
                 const unsigned salt = (unsigned)(n * (N * N + RG) + c) * 2u + f + 0x1b873593u;
                 const float o0 = f32_sr(v[0], salt);
+                // h: the rounding errors carried from one deviation to the next
+                // (mass_encode), in FP64 here
+                double e = 0.0;
+                unsigned short w[8];
+#pragma unroll
+                for (int q = 2; q <= 9; ++q) {
+                    const double xv = (v[q - 1] - (double)rq(q) * (double)o0) * sc - e;
+                    w[q - 2] = enc_sr<FMT>((float)xv, salt + 7u * q);
+                    if (f == 0) e = (double)dec<FMT>(w[q - 2]) - xv;
+                }
                 if (interior) {
                     (f ? m.B1g : m.B1h)[(size_t)n * G.bplane + (size_t)(y - 1) * N + (x - 1)] = o0;
 #pragma unroll
-                    for (int q = 2; q <= 9; ++q)
-                        (f ? m.Bdg : m.Bdh)[G.bb(n, q, x, y)] =
-                            enc_sr<FMT>((float)((v[q - 1] - (double)rq(q) * (double)o0) * sc), salt + 7u * q);
+                    for (int q = 2; q <= 9; ++q) (f ? m.Bdg : m.Bdh)[G.bb(n, q, x, y)] = w[q - 2];
                 } else {
                     const size_t off = G.a(n, 1, x, y);
                     (f ? m.A1g : m.A1h)[off - (size_t)8 * G.aplane * n] = o0;
 #pragma unroll
-                    for (int q = 2; q <= 9; ++q)
-                        (f ? m.Adg : m.Adh)[off + (size_t)(q - 1) * G.aplane] =
-                            enc_sr<FMT>((float)((v[q - 1] - (double)rq(q) * (double)o0) * sc), salt + 7u * q);
+                    for (int q = 2; q <= 9; ++q) (f ? m.Adg : m.Adh)[off + (size_t)(q - 1) * G.aplane] = w[q - 2];
                 }
             } else {
                 float w[9];
