@@ -56,6 +56,7 @@ sys.path.insert(0, PKG)
 METRIC = "MLUPS and HBM GB/s on 1 B200: mixed-prec batched vs FP64 plain at stated error"
 BYTES_PER_UPDATE = 352  # 2 * (18 populations + C, P, Ux, Uy) * 8 B
 # algorithmic bytes per leaf cell of the fused kernels (reads + writes, FP64)
+BYTES_PER_UPDATE_MIXED = 104
 KERNELS = {
     0: ("fill_c2_collide", 296),        # h,g,C in; h,g out
     1: ("fill_hg_stream_macro_h", 296), # h,g in; h,g,C out
@@ -269,6 +270,7 @@ def cpu_leg(orc, p, inner, seconds, min_chunks=0, check_after=None):
     min_chunks); after chunk `check_after[0]` its diagnostics are handed to
     check_after[1]. Returns MLUPS, chunks, seconds."""
     updates, elapsed, chunks = 0, 0.0, 0
+    ph0 = orc.phase_times()
     while chunks < min_chunks or elapsed < seconds:
         nleaf = orc.counts()["nleaf"]
         t = time.perf_counter()
@@ -279,6 +281,9 @@ def cpu_leg(orc, p, inner, seconds, min_chunks=0, check_after=None):
         if check_after and chunks == check_after[0]:
             check_after[1](orc.output())
     check_state(orc.output(), f"oracle after {chunks} intervals")
+    ph = {k: v - ph0[k] for k, v in orc.phase_times().items()}
+    tot = sum(ph.values()) or 1.0
+    cpu_leg.phase_share = {k: round(v / tot, 4) for k, v in ph.items()}
     return updates / elapsed / 1e6, chunks, elapsed
 
 
@@ -351,37 +356,6 @@ def mixed_error_report(checkpoints=(1000, 2500, 5000)):
     rep["workload"] = "rising_bubble_base64x128_blocks16_L2_R32 (density ratio 10)"
     rep["bounds"] = {"rise_velocity_rel_err": 0.01, "mass_rel_err": 1e-6}
     return rep
-
-
-def batched_leg(count=256, tune_count=32, intervals=3):
-    """Batched uneven instances: the seeded 256-problem batch, block size and
-    CTAs per SM picked by amrlbm.autotune on its first tune_count problems,
-    then the whole batch timed in FP64 and in FP16."""
-    import amrlbm
-    insts = amrlbm.batch_instances(count)
-    best, table = amrlbm.autotune(insts[:tune_count], "fp16", intervals=1, warmup=1)
-    n = best["block"] if best else 16
-    run = amrlbm.rescale_instances(insts, 16, n)
-    g = amrlbm.AmrLbm(amrlbm.batch_params(n=n, max_blks=400000), instances=run)
-    g.initialize_rising_bubble()
-    c = g.counts()
-    res = {"instances": count, "block": f"{n}x{n}", "leaves": c["nleaf"],
-           "leaf_cells": c["nleaf"] * n * n, "autotune": {"best": best, "table": table}}
-    for _ in range(2):
-        g.main_loop(10)
-    res["fp64_mlups"] = amrlbm.time_intervals(g, intervals, 10)
-    g.set_precision("fp16")
-    g.set_launch(best["ctas_per_sm"] if best else 0)
-    for _ in range(2):
-        g.main_loop(10)
-    res["fp16_mlups"] = amrlbm.time_intervals(g, intervals, 10)
-    d = g.output_instances()
-    bad = [i for i, x in enumerate(d) if not (x["u_max"] < U_BOUND and x["rho_min"] > 0)]
-    if bad:
-        raise RuntimeError(f"batched instances {bad[:8]} not physical")
-    g.close()
-    res["fp16_vs_fp64_batched"] = res["fp16_mlups"] / res["fp64_mlups"]
-    return res
 
 
 def learned_leg(samples_target=1_000_000, eval_steps=960):
@@ -464,26 +438,36 @@ def long_run_leg(steps=5000):
     return out
 
 
-def combined_leg(net, count=256, steps=320, ctas_per_sm=0):
-    """The three layers together on the seeded 256-problem batch: FP16
-    storage, every instance in one pool and one graph per interval, the
-    learned regrid every 32 steps (the forecaster of the learned-regrid leg);
-    against the plain FP64 path on the same batch with the criterion every 10
-    steps. Both run `steps` steps from the start-up, device-timed; per
-    instance, the relative mass and rise-velocity differences at the end."""
+def batched_leg(net, count=256, steps=2000, tune_count=32):
+    """Batched uneven instances, and the three layers together: the seeded
+    256-problem batch (block size and CTAs per SM picked by amrlbm.autotune
+    on its first tune_count problems), each run `steps` steps from the
+    start-up, device-timed: the plain FP64 path with the criterion every 10
+    steps; FP16 storage with the criterion every 10 steps; FP16 storage with
+    the learned regrid every 32 steps (the forecaster of the learned-regrid
+    leg). Per instance at the end, the relative mass and rise-velocity
+    differences of each FP16 run against the FP64 one."""
     import numpy as np
     import amrlbm
     insts = amrlbm.batch_instances(count)
-    res = {"instances": count, "steps": steps}
+    best, table = amrlbm.autotune(insts[:tune_count], "fp16", intervals=1, warmup=1)
+    ctas = (best or {}).get("ctas_per_sm", 0)
+    res = {"instances": count, "steps": steps, "block": "16x16",
+           "autotune": {"best": best, "table": table}}
     ends = {}
-    for name, prec, every, use in (("fp64_criterion_every_10", "fp64", 10, False),
-                                   ("fp16_learned_every_32", "fp16", 32, True)):
+    arms = (("fp64_criterion_every_10", "fp64", 10, False),
+            ("fp16_criterion_every_10", "fp16", 10, False),
+            ("fp16_learned_every_32", "fp16", 32, True))
+    for name, prec, every, use in arms:
         g = amrlbm.AmrLbm(amrlbm.batch_params(n=16, max_blks=400000, regrid_every=every),
                           instances=insts)
         g.initialize_rising_bubble()
+        c = g.counts()
+        res.setdefault("leaves_start", c["nleaf"])
+        res.setdefault("leaf_cells_start", c["nleaf"] * 256)
         if prec != "fp64":
             g.set_precision(prec)
-            g.set_launch(ctas_per_sm)
+            g.set_launch(ctas)
         if use:
             g.set_regrid_net(net, horizon=16.0, threshold=0.5)
         c0 = g.profile_read(0)[2]
@@ -493,22 +477,26 @@ def combined_leg(net, count=256, steps=320, ctas_per_sm=0):
         ms = g.timer_stop()
         st = g.regrid_stats()
         st["mlups"] = (g.profile_read(0)[2] - c0) / (ms / 1e3) / 1e6
+        st["ms"] = ms
         st["leaves"] = g.counts()["nleaf"]
         d = g.output_instances()
         bad = [i for i, x in enumerate(d) if not (x["u_max"] < U_BOUND and x["rho_min"] > 0)]
         if bad:
-            raise RuntimeError(f"{name}: instances {bad[:8]} not physical")
+            raise RuntimeError(f"batched {name}: instances {bad[:8]} not physical")
         ends[name] = d
         res[name] = st
         g.close()
-    a, b = ends["fp64_criterion_every_10"], ends["fp16_learned_every_32"]
-    dm = np.array([abs(y["mass"] - x["mass"]) / abs(x["mass"]) for x, y in zip(a, b)])
-    dv = np.array([abs(y["rise_velocity"] - x["rise_velocity"]) / max(abs(x["rise_velocity"]), 1e-300)
-                   for x, y in zip(a, b)])
-    res["mass_rel_diff"] = {"max": float(dm.max()), "median": float(np.median(dm))}
-    res["rise_velocity_rel_diff"] = {"max": float(dv.max()), "median": float(np.median(dv)),
-                                     "instances_within_1pct": int((dv <= 0.01).sum())}
-    res["speedup"] = res["fp16_learned_every_32"]["mlups"] / res["fp64_criterion_every_10"]["mlups"]
+    ref = ends["fp64_criterion_every_10"]
+    for name in ("fp16_criterion_every_10", "fp16_learned_every_32"):
+        dm = np.array([abs(y["mass"] - x["mass"]) / abs(x["mass"]) for x, y in zip(ref, ends[name])])
+        dv = np.array([abs(y["rise_velocity"] - x["rise_velocity"]) /
+                       max(abs(x["rise_velocity"]), 1e-300) for x, y in zip(ref, ends[name])])
+        res[name]["vs_fp64"] = {
+            "mass_rel_diff": {"max": float(dm.max()), "median": float(np.median(dm)),
+                              "instances_within_1e-6": int((dm <= 1e-6).sum())},
+            "rise_velocity_rel_diff": {"max": float(dv.max()), "median": float(np.median(dv)),
+                                       "instances_within_1pct": int((dv <= 0.01).sum())}}
+        res[name]["speedup_vs_fp64"] = res[name]["mlups"] / res["fp64_criterion_every_10"]["mlups"]
     return res
 
 
@@ -634,7 +622,9 @@ def run_own(args):
             gpu.set_precision(prec)
             for _ in range(2):
                 gpu.main_loop(inner)
-            mixed[prec] = {"mlups": amrlbm.time_intervals(gpu, args.steps, inner)}
+            v = amrlbm.time_intervals(gpu, args.steps, inner)
+            # compulsory traffic with 16-bit populations and FP32 fields: 2 (18 x 2 + 4 x 4) B
+            mixed[prec] = {"mlups": v, "hbm_gbs": v * 1e6 * BYTES_PER_UPDATE_MIXED / 1e9}
             check_state(gpu.output(), f"{prec} leg")
         gpu.set_precision("fp64")
         mixed["fp64_mlups"] = value
@@ -677,20 +667,21 @@ def run_own(args):
                "sample": f"{chunks} x {inner} time steps from the state the timed region "
                          f"started from ({el:.1f} s); after the first {args.steps} "
                          f"intervals its diagnostics equalled the device's bit for bit",
-               "parity_over_timed_window": "bit-exact"}
+               "parity_over_timed_window": "bit-exact",
+               "phase_share": cpu_leg.phase_share}
         orc.set_threads(4)
         v4, chunks4, el4 = cpu_leg(orc, p, inner, args.cpu_seconds / 2)
         cpu4 = {"value": v4, "unit": "MLUPS", "cores": 4, "kind": "port",
                 "sample": f"the next {chunks4} x {inner} time steps ({el4:.1f} s) at 4 threads, "
-                          f"the reference's OMP_NUM_THREADS"}
+                          f"the reference's OMP_NUM_THREADS",
+                "phase_share": cpu_leg.phase_share}
         orc.close()
-    mixed_err = batched = learned = combined = None
+    mixed_err = batched = learned = None
     long_run = long_run_leg()
     if not args.no_mixed:
         mixed_err = mixed_error_report()
-        batched = batched_leg()
         learned, net = learned_leg()
-        combined = combined_leg(net, ctas_per_sm=(batched["autotune"]["best"] or {}).get("ctas_per_sm", 0))
+        batched = batched_leg(net)
         net.close()
     line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
@@ -701,7 +692,7 @@ def run_own(args):
             "e2e": e2e, "clocks": clk,
             "gpu_launches": int(launches), "kernels": kernels,
             "mixed_precision": mixed or None, "mixed_precision_error": mixed_err,
-            "batched": batched, "learned_regrid": learned, "combined": combined,
+            "batched": batched, "learned_regrid": learned,
             "long_run": long_run,
             "leaf_cells_per_step": updates / (args.steps * inner),
             "diagnostics": {k: diag[k] for k in ("mass", "y_centroid", "rise_velocity")}}

@@ -85,6 +85,10 @@ struct orc_sim {
     amrlbm_params prm;
     Phys ph;
     int nx, ny, MaxBlks, nthreads;
+    /* seconds per phase, as the timers of Main_Loop (AMR_Rising_2D_OMP.f90:
+     * 366-375): Macroscopic_h, Macroscopic_g, collision, advection, Ghost_C,
+     * Ghost_C2, Ghost_hg, refine */
+    double phase_s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     std::vector<Block> blk; /* 1-based */
     int Nblks = 0, nLeaf = 0, KK = 0, LevelMin = 0, LevelMax = 0;
     std::vector<int> LeafBlks;
@@ -1520,26 +1524,42 @@ void initialize_rising_bubble(orc_sim& s) {
 
 /* one iteration of the Main_Loop body (AMR_Rising_2D_OMP.f90:304-363) */
 int main_loop_step(orc_sim& s) {
+    double t = omp_get_wtime();
+    auto lap = [&](int k) {  /* phase k's timer (Main_Loop, :316-362) */
+        const double t2 = omp_get_wtime();
+        s.phase_s[k] += t2 - t;
+        t = t2;
+    };
     determine_min_max_levels(s);
     fill_ghost_cells_c(s, 2);
+    lap(5);
     /* Phase_Field_LBM_h_g_AMR (:381-430) */
 #pragma omp parallel for schedule(static) num_threads(s.nthreads)
     for (int m = 0; m < s.nLeaf; ++m) collision(s, s.blk[s.LeafBlks[m]]);
+    lap(2);
     fill_ghost_cells_hg(s);
+    lap(6);
 #pragma omp parallel for schedule(static) num_threads(s.nthreads)
     for (int m = 0; m < s.nLeaf; ++m) {
         Block& B = s.blk[s.LeafBlks[m]];
         stream_field(s, B.h, B.dx);
         stream_field(s, B.g, B.dx);
     }
+    lap(3);
 #pragma omp parallel for schedule(static) num_threads(s.nthreads)
     for (int m = 0; m < s.nLeaf; ++m) macro_h(s, s.blk[s.LeafBlks[m]]);
+    lap(0);
     fill_ghost_cells_c(s, 1);
+    lap(4);
 #pragma omp parallel for schedule(static) num_threads(s.nthreads)
     for (int m = 0; m < s.nLeaf; ++m) macro_g(s, s.blk[s.LeafBlks[m]]);
+    lap(1);
     s.stepcount++;
-    if (s.stepcount % s.prm.regrid_every == 0)
-        return refine_derefine_mesh(s, s.prm.refin_tol, s.prm.deref_tol);
+    if (s.stepcount % s.prm.regrid_every == 0) {
+        const int r = refine_derefine_mesh(s, s.prm.refin_tol, s.prm.deref_tol);
+        lap(7);
+        return r;
+    }
     return s.err;
 }
 
@@ -1624,6 +1644,10 @@ int orc_init_rising_bubble(orc_sim* s) {
 int orc_init_fields(orc_sim* s) {
     initialize_rising_bubble(*s);
     return s->err;
+}
+
+void orc_phase_times(const orc_sim* s, double out[8]) {
+    for (int k = 0; k < 8; ++k) out[k] = s->phase_s[k];
 }
 
 int orc_step(orc_sim* s, int nsteps) {

@@ -36,6 +36,10 @@ void orc_set_physics(orc_sim* s, const amrlbm_physics* ph);
 int orc_init_rising_bubble(orc_sim* s);
 int orc_init_fields(orc_sim* s);
 int orc_step(orc_sim* s, int nsteps);
+/* seconds spent per phase so far, in the order of Main_Loop's timer printout
+ * (AMR_Rising_2D_OMP.f90:366-375): Macroscopic_h, Macroscopic_g, collision,
+ * advection, Ghost_C, Ghost_C2, Ghost_hg, refine */
+void orc_phase_times(const orc_sim* s, double out[8]);
 
 /* Main_Loop phases */
 void orc_min_max_levels(orc_sim* s);

@@ -38,6 +38,7 @@ def lib():
             "orc_init_rising_bubble": (ct.c_int, [vp]),
             "orc_init_fields": (ct.c_int, [vp]),
             "orc_step": (ct.c_int, [vp, ct.c_int]),
+            "orc_phase_times": (None, [vp, ct.POINTER(ct.c_double)]),
             "orc_min_max_levels": (None, [vp]),
             "orc_set_level_range": (None, [vp, ct.c_int, ct.c_int]),
             "orc_fill_c2": (None, [vp]), "orc_fill_c": (None, [vp]), "orc_fill_hg": (None, [vp]),
@@ -101,6 +102,16 @@ class Oracle:
 
     def set_threads(self, n):
         self.L.orc_set_threads(self.s, n)
+
+    PHASES = ("Macroscopic_h", "Macroscopic_g", "collision", "advection", "Ghost_C", "Ghost_C2",
+              "Ghost_hg", "refine")
+
+    def phase_times(self):
+        """Seconds per phase so far, named as Main_Loop's timers
+        (AMR_Rising_2D_OMP.f90:366-375)."""
+        a = (ct.c_double * 8)()
+        self.L.orc_phase_times(self.s, a)
+        return dict(zip(self.PHASES, list(a)))
 
     def error(self):
         return self.L.orc_last_error(self.s)
