@@ -919,7 +919,12 @@ def collect_samples(sim: "AmrLbm", regrids: int, horizon: int = 16, keep_far: fl
         t = sim.topology()
         leaves = sim.leaves()
         lv = t["level"][leaves - 1]
-        cand = leaves[lv < sim.params.max_levels]
+        if sim.instances:  # each instance's own level count
+            inst = sim.block_instances()
+            maxlv = np.array([i.max_levels for i in sim.instances])[inst[leaves - 1]]
+        else:
+            maxlv = sim.params.max_levels
+        cand = leaves[lv < maxlv]
         x = sim.block_features(cand, float(horizon))
         sim.main_loop(horizon)
         err = sim.block_errors()
