@@ -203,10 +203,13 @@ __device__ __forceinline__ float foreign_cf(const int* fb, int fmax, int j, cons
 }
 
 // the C ring of width w of item k (block n) on the tile T (pool layout of
-// one block) and in memory; foreign values in Fs. Ends with a barrier.
+// one block) and in memory; foreign values in Fs. cg (level order): sources
+// through L2, since a coarser neighbour's ring is written in this launch;
+// without level order every source in memory is an interior cell that no
+// item of the launch writes. Ends with a barrier.
 template <int N>
 __device__ void ring_c(const DevState& s, const Geo<N>& G, const int* pl, int R, int w,
-                       const ItemRec& r, const float* Fs, float* T) {
+                       const ItemRec& r, const float* Fs, float* T, bool cg) {
     const float* C = s.mp.C;
     for (int e = threadIdx.x; e < r.na + r.n2 + r.n3; e += blockDim.x) {
         const int meta = pl[e];
@@ -229,7 +232,8 @@ __device__ void ring_c(const DevState& s, const Geo<N>& G, const int* pl, int R,
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
                 const unsigned wd = (unsigned)pl[(1 + i) * R + e];
-                g[i] = (kind == 3 && (wd & kIndirect)) ? Fs[wd & ~kIndirect] : __ldcg(C + wd);
+                g[i] = (kind == 3 && (wd & kIndirect)) ? Fs[wd & ~kIndirect]
+                                                        : (cg ? __ldcg(C + wd) : __ldg(C + wd));
             }
             v = combine_f(meta, g);
         }
@@ -514,7 +518,7 @@ __global__ void __launch_bounds__(N * N, (N == 16 ? 3 : 8)) k_mp_collide(const _
             for (int j = t; j < r.nf; j += blockDim.x) Fs[j] = foreign_cf(fb, s.fmax, j, m.C);
             __syncthreads();
             wait_for_coarser(s, Q_FILLC, k);
-            ring_c<N>(s, G, s.plan_c2 + (size_t)k * R * PLAN_INTS, R, 2, r, Fs, T);
+            ring_c<N>(s, G, s.plan_c2 + (size_t)k * R * PLAN_INTS, R, 2, r, Fs, T, true);
             walls_c<N>(s, G, n, 2, r.w3, r.w4, T);
             publish_ring(s, Q_FILLC, n);
             float h[9], g[9];
@@ -567,7 +571,7 @@ __global__ void __launch_bounds__(N * N, (N == 16 ? 3 : 8)) k_mp_collide(const _
         const int* fb = reinterpret_cast<const int*>(S + SL::O_FR);
         for (int j = t; j < r.nf; j += blockDim.x) Fs[j] = foreign_cf(fb, s.fmax, j, m.C);
         __syncthreads();
-        ring_c<N>(s, G, reinterpret_cast<const int*>(S + SL::O_PL), R, 2, r, Fs, T);
+        ring_c<N>(s, G, reinterpret_cast<const int*>(S + SL::O_PL), R, 2, r, Fs, T, false);
         walls_c<N>(s, G, n, 2, r.w3, r.w4, T);
         // the next item's copies, now that its record is in
         if (t < REC_WORDS) cp_async_wait_all();
@@ -679,7 +683,7 @@ __device__ void hg_item(const DevState& s, const Geo<N>& G, int k, const ItemRec
                 for (int i = 0; i < 9; ++i)
                     gg[i] = (kind == 3 && (wd[i] & kIndirect))
                                 ? Fs[(f * 9 + q - 1) * fmax + (wd[i] & ~kIndirect)]
-                                : (kind == 3 ? dec_a<N, FMT, true>(m, G, f, wd[i], q)
+                                : (kind == 3 && !fast ? dec_a<N, FMT, true>(m, G, f, wd[i], q)
                                              : dec_a<N, FMT>(m, G, f, wd[i], q));
                 As[f * FP + (q - 1) * AP + yy * (N + 2) + xx] = combine_f(meta, gg);
             }
@@ -893,7 +897,9 @@ __global__ void __launch_bounds__(N * N) k_mp_tail(const __grid_constant__ DevSt
         for (int j = t; j < r.nf; j += blockDim.x) Fs[j] = foreign_cf(fb, s.fmax, j, m.C);
         __syncthreads();
         if (!fast) wait_for_coarser(s, Q_FILLC1, k);
-        ring_c<N>(s, G, s.plan_c1 + (size_t)k * R * PLAN_INTS, R, 1, r, Fs, T);
+        // through L2 also without level order: measured faster here (the ring
+        // of one width has little reuse of its sources)
+        ring_c<N>(s, G, s.plan_c1 + (size_t)k * R * PLAN_INTS, R, 1, r, Fs, T, true);
         walls_c<N>(s, G, n, 1, r.w3, r.w4, T);
         if (!fast) publish_ring(s, Q_FILLC1, n);
         const float inv_dx = 1.f / (float)__ldg(s.dx + n);

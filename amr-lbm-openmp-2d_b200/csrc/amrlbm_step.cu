@@ -357,11 +357,14 @@ __device__ void foreign_hg(const DevState& s, const Geo<N>& G, const int* fb, in
     __syncthreads();
 }
 
-// a coarse-to-fine source: a foreign slot's value in Fs, or a cell in memory
-// (the coarser neighbour's interior, or its ring after a wait: through L2)
+// a coarse-to-fine source: a foreign slot's value in Fs, or a cell in memory.
+// cg (level order): the coarser neighbour's ring, written in this launch
+// before a wait, so through L2. Without level order every source in memory
+// is an interior cell that no item of the launch writes (the rings it could
+// read are foreign cells), and the loads may go through L1.
 __device__ __forceinline__ double c2f_source(unsigned w, const double* Fs, const double* A,
-                                             size_t qo) {
-    return (w & kIndirect) ? Fs[w & ~kIndirect] : ldcg(A + w + qo);
+                                             size_t qo, bool cg) {
+    return (w & kIndirect) ? Fs[w & ~kIndirect] : (cg ? ldcg(A + w + qo) : __ldg(A + w + qo));
 }
 
 // which plan kinds a fill pass evaluates: 0 all, 1 all but coarse-to-fine
@@ -379,7 +382,7 @@ __device__ __forceinline__ bool pass_takes(int mode, int kind) {
 template <int N>
 __device__ __forceinline__ int c_entry(const DevState& s, const Geo<N>& G, const int* pl, int R,
                                        int e, int n, int w, const double* Fs, double* T,
-                                       bool to_mem) {
+                                       bool to_mem, bool cg) {
     const int meta = pl[e];
     const int kind = plan_kind(meta);
     if (kind == 0) return 0;
@@ -402,7 +405,7 @@ __device__ __forceinline__ int c_entry(const DevState& s, const Geo<N>& G, const
             for (int i = 0; i < 9; ++i) g[i] = __ldg(s.C + (unsigned)pl[(1 + i) * R + e]);
         } else {
 #pragma unroll
-            for (int i = 0; i < 9; ++i) g[i] = c2f_source((unsigned)pl[(1 + i) * R + e], Fs, s.C, 0);
+            for (int i = 0; i < 9; ++i) g[i] = c2f_source((unsigned)pl[(1 + i) * R + e], Fs, s.C, 0, cg);
         }
         v = plan_combine(meta, g);
     }
@@ -421,7 +424,7 @@ __device__ void fill_ring_c(const DevState& s, const Geo<N>& G, int k, int n, in
     const int* pl = ((w == 2) ? s.plan_c2 : s.plan_c1) + (size_t)k * R * PLAN_INTS;
     for (int e = threadIdx.x; e < R; e += blockDim.x)
         if (pass_takes(mode, plan_kind(__ldg(pl + e))))
-            c_entry<N>(s, G, pl, R, e, n, w, Fs, nullptr, true);
+            c_entry<N>(s, G, pl, R, e, n, w, Fs, nullptr, true, true);
 }
 
 // One copied h/g ghost cell (plan entry e, field f): the 9 populations'
@@ -451,7 +454,7 @@ __device__ __forceinline__ void hg_copy(const DevState& s, const Geo<N>& G, cons
 template <int N>
 __device__ __forceinline__ void hg_interp(const DevState& s, const Geo<N>& G, const int* pl, int RG,
                                           int e, int qq, int n, const double* Fs, double* As,
-                                          bool to_mem) {
+                                          bool to_mem, bool cg) {
     const int meta = pl[e];
     const int kind = plan_kind(meta);
     int x, y;
@@ -469,7 +472,7 @@ __device__ __forceinline__ void hg_interp(const DevState& s, const Geo<N>& G, co
             for (int i = 0; i < 9; ++i) g[i] = __ldg(A + wd[i] + qo);
         } else {
 #pragma unroll
-            for (int i = 0; i < 9; ++i) g[i] = c2f_source(wd[i], Fs + (f * 9 + qq) * s.fmax, A, qo);
+            for (int i = 0; i < 9; ++i) g[i] = c2f_source(wd[i], Fs + (f * 9 + qq) * s.fmax, A, qo, cg);
         }
         const double v = plan_combine(meta, g);
         if (to_mem) A[G.a(n, qq + 1, x, y)] = v;
@@ -492,7 +495,7 @@ __device__ void fill_ring_hg(const DevState& s, const Geo<N>& G, int k, int n, i
     for (int u = threadIdx.x; u < 9 * RG; u += blockDim.x) {
         const int kind = plan_kind(__ldg(pl + u % RG));
         if (kind >= 2 && pass_takes(mode, kind))
-            hg_interp<N>(s, G, pl, RG, u % RG, u / RG, n, Fs, nullptr, true);
+            hg_interp<N>(s, G, pl, RG, u % RG, u / RG, n, Fs, nullptr, true, true);
     }
 }
 
@@ -845,7 +848,7 @@ template <int N>
 __device__ void fast_ring_c(const DevState& s, const Geo<N>& G, const int* pl, int R, int w,
                             const ItemRec& r, const double* Fs, double* T, bool to_mem) {
     for (int e = threadIdx.x; e < r.na + r.n2 + r.n3; e += blockDim.x)
-        c_entry<N>(s, G, pl, R, e, r.n, w, Fs, T, to_mem);
+        c_entry<N>(s, G, pl, R, e, r.n, w, Fs, T, to_mem, false);
     __syncthreads();
 }
 
@@ -861,7 +864,7 @@ __device__ void fast_ring_hg(const DevState& s, const Geo<N>& G, const int* pl, 
             hg_copy<N>(s, G, pl, RG, u % r.na, u / r.na, r.n, As, to_mem);
         } else {
             const int v = u - nC;
-            hg_interp<N>(s, G, pl, RG, r.na + v % nI, v / nI, r.n, Fs, As, to_mem);
+            hg_interp<N>(s, G, pl, RG, r.na + v % nI, v / nI, r.n, Fs, As, to_mem, false);
         }
     }
     __syncthreads();
