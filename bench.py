@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-long", action="store_true", help="skip the 5000-step run")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision, error-report and batched legs")
     ap.add_argument("--profile-forecast", action="store_true",
@@ -701,7 +702,7 @@ def run_own(args):
                 "phase_share": cpu_leg.phase_share}
         orc.close()
     mixed_err = batched = learned = None
-    long_run = long_run_leg()
+    long_run = None if args.no_long else long_run_leg()
     if not args.no_mixed:
         mixed_err = mixed_error_report()
         learned, net = learned_leg()
