@@ -797,6 +797,12 @@ class Net:
             self.lib.amrlbm_net_destroy(self.h)
             self.h = None
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
     def __del__(self):
         try:
             self.close()
