@@ -266,3 +266,19 @@ def test_bgk_option_changes_g_only_through_the_collision():
     same_h = all(np.array_equal(runs[0][b]["h"], runs[1][b]["h"]) for b in runs[0])
     diff_g = any(not np.array_equal(runs[0][b]["g"], runs[1][b]["g"]) for b in runs[0])
     assert same_h and diff_g
+
+
+def test_phase_timers_follow_main_loop():
+    """The oracle's per-phase timers (the CPU baseline's breakdown, as
+    Main_Loop's timers, AMR_Rising_2D_OMP.f90:366-375) all advance over steps
+    with a regrid every step."""
+    p = amrlbm.workload_small()
+    o = Oracle(p, 2)
+    o.initialize_rising_bubble()
+    t0 = o.phase_times()
+    o.main_loop(3)
+    t1 = o.phase_times()
+    o.close()
+    assert list(t1) == list(Oracle.PHASES)
+    for k in Oracle.PHASES:
+        assert t1[k] > t0[k] >= 0.0, k
