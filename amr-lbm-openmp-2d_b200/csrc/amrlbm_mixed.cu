@@ -628,9 +628,12 @@ __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wa
 // Bounce_Back_3/4, the ring to memory where asked, then
 // Perfect_Shift_AMR / Streaming_LaxWendroff_AMR (:41-90) into B and
 // Macroscopic_Values_h_AMR (:193-201)
-template <int N, int FMT>
+// (FAST: without level order, a compile-time flag so that each path gets its
+// own code)
+template <int N, int FMT, bool FAST>
 __device__ void hg_item(const DevState& s, const Geo<N>& G, int k, const ItemRec& r, const int* fb,
-                        const int* pl, float* As, float* Fs, bool fast, bool wr) {
+                        const int* pl, float* As, float* Fs, bool wr) {
+    constexpr bool fast = FAST;
     constexpr int AP = (N + 2) * (N + 2), FP = 9 * AP;
     const int t = threadIdx.x, n = r.n, RG = ring1_len(N, N), fmax = s.fmax;
     const MpState& m = s.mp;
@@ -788,8 +791,8 @@ __global__ void __launch_bounds__(N * N, (N == 16 ? 3 : 8))
             __syncthreads();
             const ItemRec r = item_rec_of(rec[0]);
             decode_mem(r.n);
-            hg_item<N, FMT>(s, G, k, r, s.frn_hg + (size_t)k * s.fmax * FRN_INTS,
-                            s.plan_hg + (size_t)k * RG * PLAN_INTS, As, Fs, false, wr != 0);
+            hg_item<N, FMT, false>(s, G, k, r, s.frn_hg + (size_t)k * s.fmax * FRN_INTS,
+                                   s.plan_hg + (size_t)k * RG * PLAN_INTS, As, Fs, wr != 0);
         }
         queue_done(s, Q_FILLHG);
         return;
@@ -861,8 +864,8 @@ __global__ void __launch_bounds__(N * N, (N == 16 ? 3 : 8))
                 for (int q = 2; q <= 9; ++q) As[f * FP + (q - 1) * AP + c] = dec<FMT>(D[(q - 1) * AP + c]) * is + rq(q) * rest;
             }
         }
-        hg_item<N, FMT>(s, G, k, r, reinterpret_cast<const int*>(S + SL::O_FR),
-                        reinterpret_cast<const int*>(S + SL::O_PL), As, Fs, true, wr != 0);
+        hg_item<N, FMT, true>(s, G, k, r, reinterpret_cast<const int*>(S + SL::O_FR),
+                              reinterpret_cast<const int*>(S + SL::O_PL), As, Fs, wr != 0);
         __syncthreads();  // As, Fs and the stage are read before they are refilled
         if (t == 0) s_nn = n_after;
         __syncthreads();
