@@ -2,8 +2,9 @@
 
 Every test runs the same inputs through libamrlbm.so (amrlbm.AmrLbm) and the
 oracle and requires identical integer state and identical FP64 fields
-(tolerance 0: the north-star bound is 1e-12 relative; the device path meets
-it exactly because it keeps the reference's operation order without FMA).
+(tolerance 0: the FP64 path's stated bound is 1e-12 relative; the device path
+meets it exactly because it keeps the reference's operation order without
+FMA).
 """
 import numpy as np
 import pytest
