@@ -702,8 +702,10 @@ def run_own(args):
                 "phase_share": cpu_leg.phase_share}
         orc.close()
     mixed_err = batched = learned = None
-    long_run = None if args.no_long else long_run_leg()
-    if not args.no_mixed:
+    # the single-GPU legs (minutes of rank 0 alone) only at N = 1: in a
+    # scaling run the other ranks' GPUs would wait for them
+    long_run = None if (args.no_long or world > 1) else long_run_leg()
+    if not args.no_mixed and world == 1:
         mixed_err = mixed_error_report()
         learned, net = learned_leg()
         net.close()
