@@ -671,7 +671,7 @@ __device__ void hg_item(const DevState& s, const Geo<N>& G, int k, const ItemRec
 #pragma unroll
             for (int q = 0; q < 9; ++q) As[f * FP + q * AP + yy * (N + 2) + xx] = v[q];
         } else {
-            const int v2 = u - nC, e = r.na + v2 % nI, q = v2 / nI + 1;
+            const int v2 = u - nC, e = r.na + v2 / 9, q = v2 % 9 + 1;
             const int meta = pl[e];
             const int kind = plan_kind(meta);
             int xx, yy;
