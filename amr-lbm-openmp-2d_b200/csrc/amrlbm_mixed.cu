@@ -654,7 +654,8 @@ __device__ void hg_item(const DevState& s, const Geo<N>& G, int k, const ItemRec
     }
     __syncthreads();
     if (!fast) wait_for_coarser(s, Q_FILLHG, k);
-    // the ring: copies per (cell, field), interpolated cells per (cell, population)
+    // the ring: copies per (cell, field), interpolated cells per (cell, population),
+    // populations fastest, so that a cell's 9 threads share each source's rest load
     const int nC = 2 * r.na, nI = r.n2 + r.n3;
     for (int u = t; u < nC + 9 * nI; u += blockDim.x) {
         if (u < nC) {
